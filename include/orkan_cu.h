@@ -1,0 +1,105 @@
+/*
+ * orkan_cu.h - C-ABI of the sm_100a kernel layer.
+ *
+ * Plain C types only (no CUDA, torch or C99-complex types in the signatures): device
+ * buffers are void*, complex coefficient arrays are interleaved (re, im) doubles,
+ * streams are cudaStream_t passed as void* (NULL = the legacy default stream).
+ * Every function enqueues its kernel(s) on the stream and returns 0, or a nonzero
+ * cudaError_t value (launch failure, invalid argument).  Functions that return a
+ * value to the host (orkan_cu_mean, orkan_cu_matel_diag) synchronise the stream.
+ *
+ * Layout codes follow state_type_t: 0 = PURE, 1 = MIXED_PACKED, 2 = MIXED_TILED;
+ * log_tile is the LOG_TILE_DIM of the tiled layout (ignored otherwise).
+ * Local-index convention for k-qubit operators: qubits[0] is the most significant
+ * bit of the 2^k-dimensional local index (the reference test convention,
+ * test/utility/gatemat.c:178-181).
+ *
+ * The public Orkan API (state.h, gate.h, channel.h, meas.h, circ.h) is implemented on
+ * top of these calls; each entry below names the reference backends it replaces.
+ */
+#ifndef ORKAN_CU_H
+#define ORKAN_CU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* PURE 1-qubit op codes (order of reference include/gate.h:28-49). */
+enum orkan_op1 {
+    ORKAN_OP_X = 0, ORKAN_OP_Y, ORKAN_OP_Z, ORKAN_OP_H, ORKAN_OP_S, ORKAN_OP_SDG,
+    ORKAN_OP_T, ORKAN_OP_TDG, ORKAN_OP_HY, ORKAN_OP_RX, ORKAN_OP_RY, ORKAN_OP_RZ, ORKAN_OP_P
+};
+/* PURE 2-qubit op codes. */
+enum orkan_op2 { ORKAN_OP_CX = 0, ORKAN_OP_CY, ORKAN_OP_CZ, ORKAN_OP_SWAP };
+
+/* Fill every live stored element with (re, im); the tiled padding of 2^n < TILE_DIM
+ * stays untouched.  Replaces the fill loops of state_pure_plus / state_packed_plus /
+ * state_tiled_plus (reference src/state/state_pure.c:30-43, state_packed.c:57-76,
+ * state_tiled.c:84-114). */
+int orkan_cu_fill(int layout, unsigned log_tile, void *data, unsigned n, double re, double im, void *stream);
+
+/* 1-qubit gate on a statevector: op in orkan_op1; c, s as the reference host code
+ * computes them (cos/sin of theta/2 for RX/RY/RZ, of theta for P; ignored otherwise).
+ * Replaces x_pure ... p_pure (reference src/gate/gate_pure.c:125-268). */
+int orkan_cu_pure_gate1(void *psi, unsigned n, unsigned target, int op, double c, double s, void *stream);
+
+/* CX / CY / CZ (qa = control, qb = target) or SWAP (qa, qb) on a statevector.
+ * Replaces cx_pure / cy_pure / cz_pure / swap_pure (reference gate_pure.c:282-396). */
+int orkan_cu_pure_gate2(void *psi, unsigned n, unsigned qa, unsigned qb, int op, void *stream);
+
+/* Toffoli on a statevector.  Replaces ccx_pure (reference gate_pure.c:405-434). */
+int orkan_cu_pure_ccx(void *psi, unsigned n, unsigned c1, unsigned c2, unsigned t, void *stream);
+
+/* rho -> U rho U^dagger for a dense k-qubit U (k = 1 or 2), u = 2^k x 2^k row-major
+ * interleaved complex.  Replaces h/hy/rx/ry_{packed,tiled} and the generic
+ * single_from_mat / two_from_mat (reference gate_packed_1q.c:126-677,
+ * gate_tiled_{h,hy,rx,ry}.c, gate_tiled_1q.c:3-184, gate_tiled_2q.c:3). */
+int orkan_cu_dm_unitary(int layout, unsigned log_tile, void *rho, unsigned n, unsigned k,
+                        const unsigned *qubits, const double *u, void *stream);
+
+/* rho -> U rho U^dagger for a monomial U with involutive permutation:
+ * (U psi)[y] = phase[y] psi[src[y]] on the k-qubit local index (k = 1..3), src[src[y]] == y.
+ * Replaces x/y_{packed,tiled}, cx/cy/swap/ccx_{packed,tiled} (reference
+ * gate_packed_{cx,cy,swap,ccx}.c, gate_tiled_{x,y,cx,cy,swap,ccx}.c). */
+int orkan_cu_dm_monomial(int layout, unsigned log_tile, void *rho, unsigned n, unsigned k,
+                         const unsigned *qubits, const unsigned *src, const double *phase, void *stream);
+
+/* rho_rc *= phi(r) conj(phi(c)) for a diagonal k-qubit gate phi(x) = phase[local(x)]
+ * (k = 1..3).  Replaces z/s/sdg/t/tdg/p/rz_{packed,tiled} and cz_{packed,tiled}
+ * (reference gate_packed_1q.c:481-523, gate_packed_cz.c:23-80, gate_tiled_{z,s,t,p,rz,cz}.c). */
+int orkan_cu_dm_phase(int layout, unsigned log_tile, void *rho, unsigned n, unsigned k,
+                      const unsigned *qubits, const double *phase, void *stream);
+
+/* 1-qubit channel: vec(rho_2x2)' = sop vec(rho_2x2), sop 4x4 row-major interleaved
+ * complex, vec order (00, 01, 10, 11).  Replaces channel_packed_1q / channel_tiled_1q
+ * (reference src/channel/channel_packed.c:48-120, channel_tiled.c:52-185). */
+int orkan_cu_dm_superop1(int layout, unsigned log_tile, void *rho, unsigned n, unsigned target,
+                         const double *sop, void *stream);
+
+/* exp_diag with a DEVICE diag array of 2^n doubles.  Replaces exp_diag_pure /
+ * exp_diag_packed / exp_diag_tiled (reference src/circ/circ_pure.c:21-33,
+ * circ_packed.c:28-71, circ_tiled.c:25-105).  t == 0 is a no-op. */
+int orkan_cu_exp_diag(int layout, unsigned log_tile, void *data, unsigned n, const double *diag,
+                      double t, void *stream);
+
+/* mean with a DEVICE obs array; *result receives the value (host pointer).  Replaces
+ * mean_pure / mean_packed / mean_tiled (reference src/meas/meas_pure.c:20-30,
+ * meas_packed.c:23-51, meas_tiled.c:29-69). */
+int orkan_cu_mean(int layout, unsigned log_tile, const void *data, unsigned n, const double *obs,
+                  double *result, void *stream);
+
+/* matel_diag on statevectors with a DEVICE obs array; result[0..1] = (re, im).
+ * Replaces matel_diag_pure (reference src/meas/meas_pure.c:32-46). */
+int orkan_cu_matel_diag(const void *bra, const void *ket, unsigned n, const double *obs,
+                        double *result, void *stream);
+
+/* Number of kernels this library has launched in this process (all devices). */
+unsigned long long orkan_cu_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ORKAN_CU_H */

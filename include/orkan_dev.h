@@ -1,0 +1,43 @@
+/*
+ * orkan_dev.h - extensions of the device build (no counterpart in the reference API,
+ * which keeps state data in host memory and lets callers read state_t.data directly).
+ */
+#ifndef ORKAN_DEV_H
+#define ORKAN_DEV_H
+
+#include "state.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* LOG_TILE_DIM this library was built with (the tiled layout's tile side is 2^value). */
+int orkan_log_tile_dim(void);
+
+/* Stream all calls are enqueued on (a cudaStream_t; NULL = the legacy default stream,
+ * the initial setting).  Calls that return host values synchronise this stream. */
+void orkan_set_stream(void *stream);
+void *orkan_get_stream(void);
+
+/* Wait until all work enqueued by the library on its stream has finished. */
+void orkan_sync(void);
+
+/* Bulk copies of the whole storage (state_len(state) elements) between the device
+ * state and a host buffer.  Return 0 on success, a cudaError_t value otherwise.
+ * orkan_state_upload does not take ownership of host (compare state_init). */
+int orkan_state_upload(state_t *state, const cplx_t *host);
+int orkan_state_download(const state_t *state, cplx_t *host);
+
+/* Kernels launched by the library so far in this process. */
+unsigned long long orkan_launch_count(void);
+
+/* Test hook: make the next n device allocations of state storage fail, as an
+ * out-of-memory device would (state_init / state_plus / state_cp then leave
+ * data == NULL with a message on stderr, as the reference does on OOM). */
+void orkan_debug_fail_allocs(int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ORKAN_DEV_H */

@@ -1,0 +1,366 @@
+// dm_engine.cuh - rho -> U rho U^dagger (and 1-qubit superoperators) on the packed and
+// tiled density-matrix layouts, as one fused row-and-column update per block of the
+// matrix staged in shared memory.
+//
+// Reference behaviour followed: the 2x2-block update of src/gate/packed/gate_packed_1q.c:65-104
+// (conjugate read/write of elements that fall in the upper triangle), the three tiled
+// sub-cases of src/gate/tiled/gate_tiled_h.c:28-223 (all-lower quads, mirrored T(tc1,tr0)
+// access, diagonal tile pair with mirror writes) and the superoperator block update of
+// src/channel/channel_packed.c:48-120 / channel_tiled.c:52-185.
+//
+// Design.  A gate acts on k <= 3 qubits.  The matrix is cut into S x S sub-tiles
+// (S = 2^ls).  Gate qubits below ls act inside a sub-tile; the h gate qubits at or
+// above ls pair up sub-tiles.  One work item ("super-tile") is the set of rows
+// R_a = (rowbase | offset(a)) * S + [0,S) and columns C_b likewise, a,b in [0, 2^h):
+// it is closed under the gate's action on rows and on columns.  The item is staged in
+// shared memory as a dense V x V block (V = S * 2^h) of the full Hermitian matrix:
+// sub-tiles stored in the lower triangle are copied, sub-tiles of the upper triangle
+// are filled with the conjugate transpose of their stored partner, and diagonal
+// sub-tiles are completed from their lower half.  Threads then apply the gate to
+// disjoint element groups of the block (no cross-thread hazards), and the stored
+// sub-tiles are written back, regenerating the upper half of every diagonal tile of
+// the tiled layout from its lower half, so the tiled mirror invariant holds exactly.
+//
+// Ownership: item (u, v), u >= v, owns every stored sub-tile whose segment indices,
+// with the high gate bits cleared, are (u, v) or (v, u); each stored element is read
+// once and written once per launch (the CPU emulator in tests/emu checks this).
+#pragma once
+
+#include "common.cuh"
+#include <math.h>
+
+namespace orkan {
+
+constexpr unsigned kDmThreads = 256;
+constexpr unsigned kDmMaxV = 64;            // largest virtual block side
+constexpr unsigned kDmMaxElems = kDmMaxV * kDmMaxV;
+
+// Geometry of one launch (computed on the host by dm_geometry()).
+struct DmGeom {
+    idx_t d;            // 2^n
+    unsigned n;
+    unsigned ls;        // log2 of the sub-tile side S
+    unsigned h;         // gate qubits with position >= ls
+    unsigned hb[3];     // their positions in segment-index space (q - ls), ascending
+    unsigned k;         // gate qubits
+    unsigned vbit[3];   // virtual-index bit of gate qubit j; j = 0 is the MSB of the local index
+    idx_t nbase;        // base segments per dimension: (d >> ls) >> h
+    idx_t items;        // nbase * (nbase + 1) / 2
+    ORKAN_HD unsigned S() const { return 1u << ls; }
+    ORKAN_HD unsigned V() const { return 1u << (ls + h); }
+    ORKAN_HD unsigned P() const { return V() + 1; }    // smem row pitch (padded)
+};
+
+// Choose the sub-tile side: the largest S (<= smax) with V^2 <= kDmMaxElems.
+// qubits[j] is gate qubit j, qubits[0] the most significant bit of the local index.
+inline bool dm_geometry(unsigned n, unsigned k, const unsigned* qubits, unsigned ls_max, DmGeom* g) {
+    if (k < 1 || k > 3 || n < k) return false;
+    for (unsigned j = 0; j < k; ++j) {
+        if (qubits[j] >= n) return false;
+        for (unsigned i = 0; i < j; ++i) if (qubits[i] == qubits[j]) return false;
+    }
+    unsigned ls = ls_max < n ? ls_max : n;
+    for (;; --ls) {
+        unsigned h = 0;
+        for (unsigned j = 0; j < k; ++j) h += (qubits[j] >= ls);
+        if ((1ull << (2 * (ls + h))) <= kDmMaxElems || ls == 0) {
+            g->d = idx_t(1) << n;
+            g->n = n;
+            g->ls = ls;
+            g->h = h;
+            g->k = k;
+            // high qubits in ascending order -> hb, and their virtual bits ls + rank
+            unsigned hq[3], nh = 0;
+            for (unsigned j = 0; j < k; ++j) if (qubits[j] >= ls) hq[nh++] = qubits[j];
+            for (unsigned a = 0; a < nh; ++a)
+                for (unsigned b = a + 1; b < nh; ++b)
+                    if (hq[b] < hq[a]) { unsigned t = hq[a]; hq[a] = hq[b]; hq[b] = t; }
+            for (unsigned a = 0; a < 3; ++a) g->hb[a] = a < nh ? hq[a] - ls : 0;
+            for (unsigned j = 0; j < k; ++j) {
+                if (qubits[j] < ls) {
+                    g->vbit[j] = qubits[j];
+                } else {
+                    unsigned rank = 0;
+                    while (hq[rank] != qubits[j]) ++rank;
+                    g->vbit[j] = ls + rank;
+                }
+            }
+            for (unsigned j = k; j < 3; ++j) g->vbit[j] = 0;
+            g->nbase = (g->d >> ls) >> h;
+            g->items = g->nbase * (g->nbase + 1) / 2;
+            return true;
+        }
+        if (ls == 0) return false;
+    }
+}
+
+// Row/column segment origins of one work item.
+struct DmItem {
+    idx_t rseg[8];
+    idx_t cseg[8];
+    bool diag;          // row base == column base
+};
+
+ORKAN_HD void dm_item(const DmGeom& g, idx_t w, DmItem& it) {
+    idx_t u, v;
+    tri_unrank(w, &u, &v);
+    const idx_t rb = insert0_sorted(u, g.hb, g.h);
+    const idx_t cb = insert0_sorted(v, g.hb, g.h);
+    for (unsigned a = 0; a < (1u << g.h); ++a) {
+        const idx_t off = spread_bits(a, g.hb, g.h);
+        it.rseg[a] = (rb | off) << g.ls;
+        it.cseg[a] = (cb | off) << g.ls;
+    }
+    it.diag = (u == v);
+}
+
+// Sub-tile classes of position (a, b) of an item.
+enum : int { kSubDirect = 0, kSubDiag = 1, kSubTransposed = 2, kSubSkip = 3 };
+
+ORKAN_HD int dm_sub_class(const DmItem& it, unsigned a, unsigned b) {
+    const idx_t R = it.rseg[a], C = it.cseg[b];
+    if (R > C) return kSubDirect;
+    if (R == C) return kSubDiag;
+    return it.diag ? kSubSkip : kSubTransposed;
+}
+
+// Element (i, j) of the stored sub-tile visited by flat index e, so that consecutive
+// e walk the layout's contiguous direction.
+template <class Map>
+ORKAN_HD void dm_line_pos(unsigned e, unsigned ls, unsigned* i, unsigned* j) {
+    const unsigned line = e >> ls, pos = e & ((1u << ls) - 1);
+    if (Map::kRowContig) { *i = pos; *j = line; } else { *i = line; *j = pos; }
+}
+
+// Stage one item into the shared block vb (pitch P).
+template <class Map, class Mem>
+ORKAN_HD void dm_load(const Mem& mem, const Map& map, const DmGeom& g, const DmItem& it,
+                      double2* vb, unsigned tid, unsigned nthr) {
+    const unsigned S = g.S(), P = g.P(), ls = g.ls, h = g.h;
+    const unsigned total = 1u << (2 * (ls + h));
+    for (unsigned f = tid; f < total; f += nthr) {
+        const unsigned pos = f >> (2 * ls), e = f & ((1u << (2 * ls)) - 1);
+        const unsigned a = pos >> h, b = pos & ((1u << h) - 1);
+        unsigned i, j;
+        dm_line_pos<Map>(e, ls, &i, &j);
+        const idx_t R = it.rseg[a], C = it.cseg[b];
+        switch (dm_sub_class(it, a, b)) {
+            case kSubDirect: {
+                const double2 v = mem.ld(map.at(R + i, C + j));
+                vb[(a * S + i) * P + b * S + j] = v;
+                if (it.diag) vb[(b * S + j) * P + a * S + i] = cconj(v);
+                break;
+            }
+            case kSubDiag: {
+                if (i >= j) {
+                    const double2 v = mem.ld(map.at(R + i, R + j));
+                    vb[(a * S + i) * P + a * S + j] = v;
+                    if (i > j) vb[(a * S + j) * P + a * S + i] = cconj(v);
+                }
+                break;
+            }
+            case kSubTransposed: {
+                // stored partner (C, R): its element (i, j) is virtual (R + j, C + i), conjugated
+                const double2 v = mem.ld(map.at(C + i, R + j));
+                vb[(a * S + j) * P + b * S + i] = cconj(v);
+                break;
+            }
+            default:
+                break;
+        }
+    }
+}
+
+// Write one item back (inverse of dm_load), regenerating tiled mirrors.
+template <class Map, class Mem>
+ORKAN_HD void dm_store(const Mem& mem, const Map& map, const DmGeom& g, const DmItem& it,
+                       const double2* vb, unsigned tid, unsigned nthr) {
+    const unsigned S = g.S(), P = g.P(), ls = g.ls, h = g.h;
+    const unsigned total = 1u << (2 * (ls + h));
+    for (unsigned f = tid; f < total; f += nthr) {
+        const unsigned pos = f >> (2 * ls), e = f & ((1u << (2 * ls)) - 1);
+        const unsigned a = pos >> h, b = pos & ((1u << h) - 1);
+        unsigned i, j;
+        dm_line_pos<Map>(e, ls, &i, &j);
+        const idx_t R = it.rseg[a], C = it.cseg[b];
+        switch (dm_sub_class(it, a, b)) {
+            case kSubDirect: {
+                const double2 v = vb[(a * S + i) * P + b * S + j];
+                mem.st(map.at(R + i, C + j), v);
+                if (Map::kMirrors && map.same_storage_block(R, C)) mem.st(map.at(C + j, R + i), cconj(v));
+                break;
+            }
+            case kSubDiag: {
+                if (i >= j) {
+                    mem.st(map.at(R + i, R + j), vb[(a * S + i) * P + a * S + j]);
+                } else if (Map::kMirrors) {
+                    mem.st(map.at(R + i, R + j), cconj(vb[(a * S + j) * P + a * S + i]));
+                }
+                break;
+            }
+            case kSubTransposed: {
+                const double2 v = vb[(a * S + j) * P + b * S + i];
+                mem.st(map.at(C + i, R + j), cconj(v));
+                if (Map::kMirrors && map.same_storage_block(C, R)) mem.st(map.at(R + j, C + i), v);
+                break;
+            }
+            default:
+                break;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Group operations on the staged block.  Each thread owns whole groups, so compute
+// needs no synchronisation between threads.
+// ---------------------------------------------------------------------------------
+
+// Virtual index with the local-index bits of gate qubits j placed (j = 0 is the MSB).
+ORKAN_HD unsigned dm_set_local(unsigned x, unsigned loc, const unsigned* vbit, unsigned k) {
+    for (unsigned j = 0; j < k; ++j) {
+        const unsigned bit = (loc >> (k - 1 - j)) & 1u;
+        x = (x & ~(1u << vbit[j])) | (bit << vbit[j]);
+    }
+    return x;
+}
+ORKAN_HD unsigned dm_get_local(unsigned x, const unsigned* vbit, unsigned k) {
+    unsigned loc = 0;
+    for (unsigned j = 0; j < k; ++j) loc = (loc << 1) | ((x >> vbit[j]) & 1u);
+    return loc;
+}
+
+// Dense 1-qubit unitary U (row-major u[2*r + c]):  G' = U G U^dagger on 2x2 groups.
+struct OpMix1 {
+    double2 u[4];
+    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
+        const unsigned V = g.V(), P = g.P(), half = V >> 1, vbq = g.vbit[0];
+        const unsigned groups = half * half;
+        for (unsigned t = tid; t < groups; t += nthr) {
+            const unsigned r0 = (unsigned)insert0(t / half, vbq), c0 = (unsigned)insert0(t % half, vbq);
+            const unsigned r1 = r0 | (1u << vbq), c1 = c0 | (1u << vbq);
+            const double2 x00 = vb[r0 * P + c0], x01 = vb[r0 * P + c1];
+            const double2 x10 = vb[r1 * P + c0], x11 = vb[r1 * P + c1];
+            // rows: Y = U X
+            const double2 y00 = cadd(cmul(u[0], x00), cmul(u[1], x10));
+            const double2 y01 = cadd(cmul(u[0], x01), cmul(u[1], x11));
+            const double2 y10 = cadd(cmul(u[2], x00), cmul(u[3], x10));
+            const double2 y11 = cadd(cmul(u[2], x01), cmul(u[3], x11));
+            // columns: Z = Y U^dagger, Z[i][j] = sum_m Y[i][m] conj(U[j][m])
+            vb[r0 * P + c0] = cadd(cmulc(y00, u[0]), cmulc(y01, u[1]));
+            vb[r0 * P + c1] = cadd(cmulc(y00, u[2]), cmulc(y01, u[3]));
+            vb[r1 * P + c0] = cadd(cmulc(y10, u[0]), cmulc(y11, u[1]));
+            vb[r1 * P + c1] = cadd(cmulc(y10, u[2]), cmulc(y11, u[3]));
+        }
+    }
+};
+
+// Dense 2-qubit unitary U (row-major u[4*r + c], local index = 2*bit(q0) + bit(q1)).
+struct OpMix2 {
+    double2 u[16];
+    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
+        const unsigned V = g.V(), P = g.P(), quarter = V >> 2;
+        unsigned asc[2] = {g.vbit[0] < g.vbit[1] ? g.vbit[0] : g.vbit[1],
+                           g.vbit[0] < g.vbit[1] ? g.vbit[1] : g.vbit[0]};
+        const unsigned groups = quarter * quarter;
+        for (unsigned t = tid; t < groups; t += nthr) {
+            const unsigned rb = (unsigned)insert0_sorted(t / quarter, asc, 2);
+            const unsigned cb = (unsigned)insert0_sorted(t % quarter, asc, 2);
+            unsigned ri[4], ci[4];
+            for (unsigned l = 0; l < 4; ++l) {
+                ri[l] = dm_set_local(rb, l, g.vbit, 2);
+                ci[l] = dm_set_local(cb, l, g.vbit, 2);
+            }
+            double2 y[4][4];
+            for (unsigned r = 0; r < 4; ++r)
+                for (unsigned c = 0; c < 4; ++c) {
+                    double2 acc = c2(0.0, 0.0);
+                    for (unsigned m = 0; m < 4; ++m) acc = cadd(acc, cmul(u[4 * r + m], vb[ri[m] * P + ci[c]]));
+                    y[r][c] = acc;
+                }
+            for (unsigned r = 0; r < 4; ++r)
+                for (unsigned c = 0; c < 4; ++c) {
+                    double2 acc = c2(0.0, 0.0);
+                    for (unsigned m = 0; m < 4; ++m) acc = cadd(acc, cmulc(y[r][m], u[4 * c + m]));
+                    vb[ri[r] * P + ci[c]] = acc;
+                }
+        }
+    }
+};
+
+// 1-qubit superoperator (row-major s[4*m + j]) on vec = (x00, x01, x10, x11).
+struct OpSuper1 {
+    double2 s[16];
+    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
+        const unsigned V = g.V(), P = g.P(), half = V >> 1, vbq = g.vbit[0];
+        const unsigned groups = half * half;
+        for (unsigned t = tid; t < groups; t += nthr) {
+            const unsigned r0 = (unsigned)insert0(t / half, vbq), c0 = (unsigned)insert0(t % half, vbq);
+            const unsigned r1 = r0 | (1u << vbq), c1 = c0 | (1u << vbq);
+            const unsigned idx[4] = {r0 * P + c0, r0 * P + c1, r1 * P + c0, r1 * P + c1};
+            double2 x[4];
+            for (unsigned m = 0; m < 4; ++m) x[m] = vb[idx[m]];
+            for (unsigned m = 0; m < 4; ++m) {
+                double2 acc = c2(0.0, 0.0);
+                for (unsigned j = 0; j < 4; ++j) acc = cadd(acc, cmul(s[4 * m + j], x[j]));
+                vb[idx[m]] = acc;
+            }
+        }
+    }
+};
+
+// Monomial gate U|x> with an involutive permutation (X, Y, CX, CY, SWAP, CCX ...):
+// (U psi)[y] = phase[y] * psi[src[y]] on the local index, src[src[y]] == y.
+// Element pairs (y, z) <-> (src y, src z) are 2-cycles; the thread owning the
+// smaller flat index of a pair updates both.
+struct OpMonomial {
+    unsigned src[8];
+    double2 phase[8];
+    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
+        const unsigned V = g.V(), P = g.P(), k = g.k;
+        const unsigned total = V * V;
+        for (unsigned f = tid; f < total; f += nthr) {
+            const unsigned r = f / V, c = f % V;
+            const unsigned lr = dm_get_local(r, g.vbit, k), lc = dm_get_local(c, g.vbit, k);
+            const unsigned r2 = dm_set_local(r, src[lr], g.vbit, k), c2i = dm_set_local(c, src[lc], g.vbit, k);
+            const unsigned f2 = r2 * V + c2i;
+            if (f2 < f) continue;
+            const double2 fa = cmulc(phase[lr], phase[lc]);
+            if (f2 == f) {
+                vb[r * P + c] = cmul(fa, vb[r * P + c]);
+            } else {
+                const double2 fb = cmulc(phase[src[lr]], phase[src[lc]]);
+                const double2 va = vb[r * P + c], vb2 = vb[r2 * P + c2i];
+                vb[r * P + c] = cmul(fa, vb2);
+                vb[r2 * P + c2i] = cmul(fb, va);
+            }
+        }
+    }
+};
+
+// Kernel body for one work item, split into phases separated by block barriers.
+template <class Map, class Mem, class Op>
+ORKAN_HD void dm_engine_item_phase(int phase, const Mem& mem, const Map& map, const DmGeom& g,
+                                   const Op& op, const DmItem& it, double2* vb, unsigned tid, unsigned nthr) {
+    if (phase == 0) dm_load(mem, map, g, it, vb, tid, nthr);
+    else if (phase == 1) op(g, vb, tid, nthr);
+    else dm_store(mem, map, g, it, vb, tid, nthr);
+}
+
+#ifdef __CUDACC__
+template <class Map, class Op>
+__global__ void __launch_bounds__(kDmThreads) k_dm_engine(DevMem mem, Map map, DmGeom g, Op op) {
+    extern __shared__ double2 vb[];
+    DmItem it;
+    for (idx_t w = blockIdx.x; w < g.items; w += gridDim.x) {
+        dm_item(g, w, it);
+        dm_load(mem, map, g, it, vb, threadIdx.x, blockDim.x);
+        __syncthreads();
+        op(g, vb, threadIdx.x, blockDim.x);
+        __syncthreads();
+        dm_store(mem, map, g, it, vb, threadIdx.x, blockDim.x);
+        __syncthreads();
+    }
+}
+#endif
+
+}  // namespace orkan

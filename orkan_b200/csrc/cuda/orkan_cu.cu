@@ -1,0 +1,317 @@
+// orkan_cu.cu - the C-ABI launch layer (include/orkan_cu.h): argument checks, launch
+// geometry, template dispatch, and the per-device scratch buffer used by reductions
+// and by the exp_diag phase tables.
+#include "common.cuh"
+#include "dm_engine.cuh"
+#include "dm_phase.cuh"
+#include "pure.cuh"
+#include "reduce.cuh"
+#include "scratch.cuh"
+
+#include "../../../include/orkan_cu.h"
+
+#include <atomic>
+#include <mutex>
+
+using namespace orkan;
+
+namespace {
+
+std::atomic<unsigned long long> g_launches{0};
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        cached[dev] = v;
+    }
+    return cached[dev];
+}
+
+inline unsigned grid_for(idx_t work_per_block_units, idx_t total_units, unsigned cap) {
+    idx_t g = (total_units + work_per_block_units - 1) / work_per_block_units;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (unsigned)g;
+}
+
+inline int finish_launch() {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return (int)cudaGetLastError();
+}
+
+struct Complex8 { double2 v[8]; };
+
+inline double2 ld_c(const double* p, unsigned i) { return c2(p[2 * i], p[2 * i + 1]); }
+
+// ---- density-matrix engine dispatch -------------------------------------------------
+template <class Op>
+int launch_engine_map(int layout, unsigned log_tile, void* rho, unsigned n, const DmGeom& g, const Op& op,
+                      cudaStream_t st) {
+    const size_t smem = (size_t)g.V() * g.P() * sizeof(double2);
+    const unsigned grid = grid_for(1, g.items, (unsigned)sm_count() * 32u);
+    DevMem mem{static_cast<double2*>(rho)};
+    if (layout == 1) {
+        PackedMap map{idx_t(1) << n};
+        auto kern = k_dm_engine<PackedMap, Op>;
+        static bool attr = false;
+        if (!attr) { cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024); attr = true; }
+        kern<<<grid, kDmThreads, smem, st>>>(mem, map, g, op);
+    } else {
+        TiledMap map{idx_t(1) << n, log_tile};
+        auto kern = k_dm_engine<TiledMap, Op>;
+        static bool attr = false;
+        if (!attr) { cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024); attr = true; }
+        kern<<<grid, kDmThreads, smem, st>>>(mem, map, g, op);
+    }
+    return finish_launch();
+}
+
+inline bool layout_ok(int layout, unsigned log_tile) {
+    if (layout == 1) return true;
+    if (layout == 2) return log_tile >= 1 && log_tile <= 8;
+    return false;
+}
+
+// sub-tile side limit: tiles for the tiled layout, 64 for packed
+inline unsigned ls_max_for(int layout, unsigned log_tile) { return layout == 2 ? log_tile : 6u; }
+
+template <class Factor>
+int launch_phase(int layout, unsigned log_tile, void* rho, unsigned n, const Factor& fac, cudaStream_t st) {
+    const PhaseGeom g = phase_geometry(n, layout == 2 ? log_tile : 5u);
+    const unsigned grid = grid_for(1, g.items, (unsigned)sm_count() * 32u);
+    DevMem mem{static_cast<double2*>(rho)};
+    if (layout == 1) {
+        k_dm_phase<PackedMap, Factor><<<grid, kPhaseThreads, 0, st>>>(mem, PackedMap{idx_t(1) << n}, g, fac);
+    } else {
+        k_dm_phase<TiledMap, Factor><<<grid, kPhaseThreads, 0, st>>>(mem, TiledMap{idx_t(1) << n, log_tile}, g, fac);
+    }
+    return finish_launch();
+}
+
+struct DevMemC2 {
+    const double2* p;
+    __device__ __forceinline__ double2 ld(idx_t i) const { return p[i]; }
+};
+
+__global__ void k_exp_table(const double* __restrict__ diag, idx_t dim, double t, double2* __restrict__ tab) {
+    for (idx_t x = (idx_t)blockIdx.x * blockDim.x + threadIdx.x; x < dim; x += (idx_t)gridDim.x * blockDim.x) {
+        double sn, cs;
+        sincos(diag[x] * t, &sn, &cs);
+        tab[x] = c2(cs, sn);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int orkan_cu_fill(int layout, unsigned log_tile, void* data, unsigned n, double re, double im, void* stream) {
+    if (!data || n > 62) return (int)cudaErrorInvalidValue;
+    idx_t len;
+    unsigned clt = 0;
+    idx_t cdim = 0;
+    const idx_t d = idx_t(1) << n;
+    if (layout == 0) {
+        len = d;
+    } else if (layout == 1) {
+        len = PackedMap{d}.len();
+    } else if (layout == 2 && log_tile >= 1 && log_tile <= 8) {
+        len = TiledMap{d, log_tile}.len();
+        if (d < (idx_t(1) << log_tile)) { clt = log_tile; cdim = d; }
+    } else {
+        return (int)cudaErrorInvalidValue;
+    }
+    const unsigned grid = grid_for(kPureThreads * 4, len, (unsigned)sm_count() * 8u);
+    k_fill<<<grid, kPureThreads, 0, as_stream(stream)>>>(DevMem{static_cast<double2*>(data)}, len, c2(re, im), clt,
+                                                         cdim);
+    return finish_launch();
+}
+
+int orkan_cu_pure_gate1(void* psi, unsigned n, unsigned target, int op, double c, double s, void* stream) {
+    if (!psi || n < 1 || n > 62 || target >= n || op < 0 || op >= kNumOp1) return (int)cudaErrorInvalidValue;
+    const idx_t npairs = idx_t(1) << (n - 1);
+    const unsigned grid = grid_for(kPureThreads * kVec, npairs, (unsigned)sm_count() * 8u);
+    DevMem mem{static_cast<double2*>(psi)};
+    cudaStream_t st = as_stream(stream);
+    switch (op) {
+#define ORKAN_CASE1(OPC) \
+    case OPC: k_pure1q<OPC><<<grid, kPureThreads, 0, st>>>(mem, npairs, target, c, s); break;
+        ORKAN_CASE1(kOpX) ORKAN_CASE1(kOpY) ORKAN_CASE1(kOpZ) ORKAN_CASE1(kOpH) ORKAN_CASE1(kOpS)
+        ORKAN_CASE1(kOpSdg) ORKAN_CASE1(kOpT) ORKAN_CASE1(kOpTdg) ORKAN_CASE1(kOpHy) ORKAN_CASE1(kOpRx)
+        ORKAN_CASE1(kOpRy) ORKAN_CASE1(kOpRz) ORKAN_CASE1(kOpP)
+#undef ORKAN_CASE1
+        default: return (int)cudaErrorInvalidValue;
+    }
+    return finish_launch();
+}
+
+int orkan_cu_pure_gate2(void* psi, unsigned n, unsigned qa, unsigned qb, int op, void* stream) {
+    if (!psi || n < 2 || n > 62 || qa >= n || qb >= n || qa == qb || op < 0 || op >= kNumOp2)
+        return (int)cudaErrorInvalidValue;
+    const idx_t nq = idx_t(1) << (n - 2);
+    const unsigned grid = grid_for(kPureThreads * kVec, nq, (unsigned)sm_count() * 8u);
+    DevMem mem{static_cast<double2*>(psi)};
+    cudaStream_t st = as_stream(stream);
+    switch (op) {
+        case kOpCX: k_pure2q<kOpCX><<<grid, kPureThreads, 0, st>>>(mem, nq, qa, qb); break;
+        case kOpCY: k_pure2q<kOpCY><<<grid, kPureThreads, 0, st>>>(mem, nq, qa, qb); break;
+        case kOpCZ: k_pure2q<kOpCZ><<<grid, kPureThreads, 0, st>>>(mem, nq, qa, qb); break;
+        case kOpSwap: k_pure2q<kOpSwap><<<grid, kPureThreads, 0, st>>>(mem, nq, qa, qb); break;
+        default: return (int)cudaErrorInvalidValue;
+    }
+    return finish_launch();
+}
+
+int orkan_cu_pure_ccx(void* psi, unsigned n, unsigned c1, unsigned c2q, unsigned t, void* stream) {
+    if (!psi || n < 3 || n > 62 || c1 >= n || c2q >= n || t >= n || c1 == c2q || c1 == t || c2q == t)
+        return (int)cudaErrorInvalidValue;
+    const idx_t no = idx_t(1) << (n - 3);
+    const unsigned grid = grid_for(kPureThreads * kVec, no, (unsigned)sm_count() * 8u);
+    k_pure_ccx<<<grid, kPureThreads, 0, as_stream(stream)>>>(DevMem{static_cast<double2*>(psi)}, no, c1, c2q, t);
+    return finish_launch();
+}
+
+int orkan_cu_dm_unitary(int layout, unsigned log_tile, void* rho, unsigned n, unsigned k, const unsigned* qubits,
+                        const double* u, void* stream) {
+    if (!rho || !qubits || !u || !layout_ok(layout, log_tile) || (k != 1 && k != 2) || n > 40)
+        return (int)cudaErrorInvalidValue;
+    DmGeom g;
+    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g)) return (int)cudaErrorInvalidValue;
+    if (k == 1) {
+        OpMix1 op;
+        for (unsigned i = 0; i < 4; ++i) op.u[i] = ld_c(u, i);
+        return launch_engine_map(layout, log_tile, rho, n, g, op, as_stream(stream));
+    }
+    OpMix2 op;
+    for (unsigned i = 0; i < 16; ++i) op.u[i] = ld_c(u, i);
+    return launch_engine_map(layout, log_tile, rho, n, g, op, as_stream(stream));
+}
+
+int orkan_cu_dm_monomial(int layout, unsigned log_tile, void* rho, unsigned n, unsigned k, const unsigned* qubits,
+                         const unsigned* src, const double* phase, void* stream) {
+    if (!rho || !qubits || !src || !phase || !layout_ok(layout, log_tile) || k < 1 || k > 3 || n > 40)
+        return (int)cudaErrorInvalidValue;
+    OpMonomial op;
+    const unsigned m = 1u << k;
+    for (unsigned y = 0; y < 8; ++y) { op.src[y] = y; op.phase[y] = c2(1.0, 0.0); }
+    for (unsigned y = 0; y < m; ++y) {
+        if (src[y] >= m || src[src[y]] != y) return (int)cudaErrorInvalidValue;   // must be an involution
+        op.src[y] = src[y];
+        op.phase[y] = ld_c(phase, y);
+    }
+    DmGeom g;
+    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g)) return (int)cudaErrorInvalidValue;
+    return launch_engine_map(layout, log_tile, rho, n, g, op, as_stream(stream));
+}
+
+int orkan_cu_dm_phase(int layout, unsigned log_tile, void* rho, unsigned n, unsigned k, const unsigned* qubits,
+                      const double* phase, void* stream) {
+    if (!rho || !qubits || !phase || !layout_ok(layout, log_tile) || k < 1 || k > 3 || n > 40)
+        return (int)cudaErrorInvalidValue;
+    GateFactor fac;
+    fac.k = k;
+    for (unsigned j = 0; j < 3; ++j) fac.q[j] = 0;
+    for (unsigned j = 0; j < k; ++j) {
+        if (qubits[j] >= n) return (int)cudaErrorInvalidValue;
+        fac.q[j] = qubits[j];
+    }
+    for (unsigned y = 0; y < 8; ++y) fac.phase[y] = y < (1u << k) ? ld_c(phase, y) : c2(1.0, 0.0);
+    return launch_phase(layout, log_tile, rho, n, fac, as_stream(stream));
+}
+
+int orkan_cu_dm_superop1(int layout, unsigned log_tile, void* rho, unsigned n, unsigned target, const double* sop,
+                         void* stream) {
+    if (!rho || !sop || !layout_ok(layout, log_tile) || target >= n || n > 40) return (int)cudaErrorInvalidValue;
+    OpSuper1 op;
+    for (unsigned i = 0; i < 16; ++i) op.s[i] = ld_c(sop, i);
+    DmGeom g;
+    const unsigned q[1] = {target};
+    if (!dm_geometry(n, 1, q, ls_max_for(layout, log_tile), &g)) return (int)cudaErrorInvalidValue;
+    return launch_engine_map(layout, log_tile, rho, n, g, op, as_stream(stream));
+}
+
+int orkan_cu_exp_diag(int layout, unsigned log_tile, void* data, unsigned n, const double* diag, double t,
+                      void* stream) {
+    if (!data || !diag || n > 62) return (int)cudaErrorInvalidValue;
+    if (t == 0.0) return 0;
+    cudaStream_t st = as_stream(stream);
+    const idx_t d = idx_t(1) << n;
+    if (layout == 0) {
+        const unsigned grid = grid_for(kPureThreads * kVec, d, (unsigned)sm_count() * 8u);
+        k_pure_exp_diag<<<grid, kPureThreads, 0, st>>>(DevMem{static_cast<double2*>(data)}, DevMemR{diag}, d, t);
+        return finish_launch();
+    }
+    if (!layout_ok(layout, log_tile) || n > 40) return (int)cudaErrorInvalidValue;
+    double2* tab = static_cast<double2*>(scratch_get(d * sizeof(double2)));
+    if (!tab) return (int)cudaErrorMemoryAllocation;
+    const unsigned grid = grid_for(256, d, (unsigned)sm_count() * 8u);
+    k_exp_table<<<grid, 256, 0, st>>>(diag, d, t, tab);
+    const int rc = finish_launch();
+    if (rc) return rc;
+    TableFactor<DevMemC2> fac{DevMemC2{tab}};
+    return launch_phase(layout, log_tile, data, n, fac, st);
+}
+
+int orkan_cu_mean(int layout, unsigned log_tile, const void* data, unsigned n, const double* obs, double* result,
+                  void* stream) {
+    if (!data || !obs || !result || n > 62) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = as_stream(stream);
+    const idx_t d = idx_t(1) << n;
+    const unsigned np = grid_for(kRedThreads * 4, d, kRedBlocks);
+    double* part = static_cast<double*>(scratch_get((np + 1) * sizeof(double)));
+    if (!part) return (int)cudaErrorMemoryAllocation;
+    double* out = part + np;
+    if (layout == 0) {
+        k_mean_pure_partial<<<np, kRedThreads, 0, st>>>(static_cast<const double2*>(data), obs, d, part);
+        int rc = finish_launch();
+        if (rc) return rc;
+        k_fold_partials<<<1, kRedThreads, 0, st>>>(part, np, 1, out);
+        rc = finish_launch();
+        if (rc) return rc;
+    } else if (layout == 1) {
+        k_mean_dm<PackedMap><<<1, kDiagThreads, 0, st>>>(static_cast<const double2*>(data), PackedMap{d}, obs, out);
+        const int rc = finish_launch();
+        if (rc) return rc;
+    } else if (layout_ok(layout, log_tile)) {
+        k_mean_dm<TiledMap><<<1, kDiagThreads, 0, st>>>(static_cast<const double2*>(data), TiledMap{d, log_tile}, obs,
+                                                        out);
+        const int rc = finish_launch();
+        if (rc) return rc;
+    } else {
+        return (int)cudaErrorInvalidValue;
+    }
+    cudaError_t e = cudaMemcpyAsync(result, out, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return (int)e;
+    return (int)cudaStreamSynchronize(st);
+}
+
+int orkan_cu_matel_diag(const void* bra, const void* ket, unsigned n, const double* obs, double* result,
+                        void* stream) {
+    if (!bra || !ket || !obs || !result || n > 62) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = as_stream(stream);
+    const idx_t d = idx_t(1) << n;
+    const unsigned np = grid_for(kRedThreads * 4, d, kRedBlocks);
+    double* part = static_cast<double*>(scratch_get((2 * np + 2) * sizeof(double)));
+    if (!part) return (int)cudaErrorMemoryAllocation;
+    double* out = part + 2 * np;
+    k_matel_pure_partial<<<np, kRedThreads, 0, st>>>(static_cast<const double2*>(bra),
+                                                     static_cast<const double2*>(ket), obs, d, part);
+    int rc = finish_launch();
+    if (rc) return rc;
+    k_fold_partials<<<1, kRedThreads, 0, st>>>(part, np, 2, out);
+    rc = finish_launch();
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyAsync(result, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return (int)e;
+    return (int)cudaStreamSynchronize(st);
+}
+
+unsigned long long orkan_cu_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+}  // extern "C"

@@ -1,0 +1,253 @@
+// emu.cpp - CPU emulation of the CUDA kernels' index logic -- TEST INFRASTRUCTURE ONLY.
+//
+// The kernels in orkan_b200/csrc/cuda are written as __host__ __device__ per-thread
+// (and per-phase) functions over a memory accessor.  This file instantiates the same
+// functions with a checking accessor and runs every thread of every block on the CPU,
+// with block barriers honoured by running each phase for all threads before the next.
+// The accessor rejects out-of-range indices and counts reads and writes per element, so
+// the tests can prove, before any GPU run, that every access of a launch stays inside
+// the storage and that each stored element is read and written exactly as often as the
+// layout's ownership rules require.  It is never used by the product library.
+#include "../../orkan_b200/csrc/cuda/common.cuh"
+#include "../../orkan_b200/csrc/cuda/dm_engine.cuh"
+#include "../../orkan_b200/csrc/cuda/dm_phase.cuh"
+#include "../../orkan_b200/csrc/cuda/pure.cuh"
+
+#include <stdint.h>
+#include <string.h>
+#include <vector>
+
+using namespace orkan;
+
+namespace {
+
+struct EmuMem {
+    double2* p;
+    idx_t len;
+    uint32_t* reads;
+    uint32_t* writes;
+    uint64_t* oob;
+    double2 ld(idx_t i) const {
+        if (i >= len) { ++*oob; return c2(0.0, 0.0); }
+        ++reads[i];
+        return p[i];
+    }
+    void st(idx_t i, double2 v) const {
+        if (i >= len) { ++*oob; return; }
+        ++writes[i];
+        p[i] = v;
+    }
+};
+
+struct EmuMemR {
+    const double* p;
+    idx_t len;
+    uint64_t* oob;
+    double ld(idx_t i) const {
+        if (i >= len) { ++*oob; return 0.0; }
+        return p[i];
+    }
+};
+
+struct EmuMemC2 {
+    const double2* p;
+    idx_t len;
+    uint64_t* oob;
+    double2 ld(idx_t i) const {
+        if (i >= len) { ++*oob; return c2(0.0, 0.0); }
+        return p[i];
+    }
+};
+
+constexpr unsigned kSms = 148;
+
+unsigned grid_for(idx_t per_block, idx_t total, unsigned cap) {
+    idx_t g = (total + per_block - 1) / per_block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (unsigned)g;
+}
+
+double2 ldc(const double* p, unsigned i) { return c2(p[2 * i], p[2 * i + 1]); }
+
+template <class Map, class Op>
+void run_engine(const EmuMem& mem, const Map& map, const DmGeom& g, const Op& op) {
+    const unsigned grid = grid_for(1, g.items, kSms * 32u);
+    std::vector<double2> vb((size_t)g.V() * g.P());
+    for (unsigned b = 0; b < grid; ++b) {
+        for (idx_t w = b; w < g.items; w += grid) {
+            DmItem it;
+            dm_item(g, w, it);
+            for (int phase = 0; phase < 3; ++phase)
+                for (unsigned t = 0; t < kDmThreads; ++t)
+                    dm_engine_item_phase(phase, mem, map, g, op, it, vb.data(), t, kDmThreads);
+        }
+    }
+}
+
+template <class Op>
+int engine_dispatch(int layout, unsigned log_tile, double* rho, idx_t len, unsigned n, const DmGeom& g,
+                    const Op& op, uint32_t* reads, uint32_t* writes, uint64_t* oob) {
+    EmuMem mem{reinterpret_cast<double2*>(rho), len, reads, writes, oob};
+    if (layout == 1) run_engine(mem, PackedMap{idx_t(1) << n}, g, op);
+    else run_engine(mem, TiledMap{idx_t(1) << n, log_tile}, g, op);
+    return 0;
+}
+
+unsigned ls_max_for(int layout, unsigned log_tile) { return layout == 2 ? log_tile : 6u; }
+
+template <class Factor>
+void run_phase(int layout, unsigned log_tile, const EmuMem& mem, unsigned n, const Factor& fac) {
+    const PhaseGeom g = phase_geometry(n, layout == 2 ? log_tile : 5u);
+    const unsigned grid = grid_for(1, g.items, kSms * 32u);
+    for (unsigned b = 0; b < grid; ++b)
+        for (idx_t w = b; w < g.items; w += grid)
+            for (unsigned t = 0; t < kPhaseThreads; ++t) {
+                if (layout == 1) dm_phase_item(mem, PackedMap{idx_t(1) << n}, g, fac, w, t, kPhaseThreads);
+                else dm_phase_item(mem, TiledMap{idx_t(1) << n, log_tile}, g, fac, w, t, kPhaseThreads);
+            }
+}
+
+}  // namespace
+
+extern "C" {
+
+// All entry points: data arrays are interleaved complex; reads/writes are per-element
+// counters (zeroed by the caller); *oob receives the number of out-of-range accesses.
+// Return 0, or -1 when the launch parameters are rejected (as the CUDA layer would).
+
+int emu_dm_unitary(int layout, unsigned log_tile, double* rho, uint64_t len, unsigned n, unsigned k,
+                   const unsigned* qubits, const double* u, uint32_t* reads, uint32_t* writes, uint64_t* oob) {
+    DmGeom g;
+    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g)) return -1;
+    if (k == 1) {
+        OpMix1 op;
+        for (unsigned i = 0; i < 4; ++i) op.u[i] = ldc(u, i);
+        return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
+    }
+    OpMix2 op;
+    for (unsigned i = 0; i < 16; ++i) op.u[i] = ldc(u, i);
+    return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
+}
+
+int emu_dm_monomial(int layout, unsigned log_tile, double* rho, uint64_t len, unsigned n, unsigned k,
+                    const unsigned* qubits, const unsigned* src, const double* phase, uint32_t* reads,
+                    uint32_t* writes, uint64_t* oob) {
+    OpMonomial op;
+    for (unsigned y = 0; y < 8; ++y) { op.src[y] = y; op.phase[y] = c2(1.0, 0.0); }
+    for (unsigned y = 0; y < (1u << k); ++y) { op.src[y] = src[y]; op.phase[y] = ldc(phase, y); }
+    DmGeom g;
+    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g)) return -1;
+    return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
+}
+
+int emu_dm_superop1(int layout, unsigned log_tile, double* rho, uint64_t len, unsigned n, unsigned target,
+                    const double* sop, uint32_t* reads, uint32_t* writes, uint64_t* oob) {
+    OpSuper1 op;
+    for (unsigned i = 0; i < 16; ++i) op.s[i] = ldc(sop, i);
+    DmGeom g;
+    const unsigned q[1] = {target};
+    if (!dm_geometry(n, 1, q, ls_max_for(layout, log_tile), &g)) return -1;
+    return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
+}
+
+int emu_dm_phase(int layout, unsigned log_tile, double* rho, uint64_t len, unsigned n, unsigned k,
+                 const unsigned* qubits, const double* phase, uint32_t* reads, uint32_t* writes, uint64_t* oob) {
+    GateFactor fac;
+    fac.k = k;
+    for (unsigned j = 0; j < 3; ++j) fac.q[j] = j < k ? qubits[j] : 0;
+    for (unsigned y = 0; y < 8; ++y) fac.phase[y] = y < (1u << k) ? ldc(phase, y) : c2(1.0, 0.0);
+    EmuMem mem{reinterpret_cast<double2*>(rho), len, reads, writes, oob};
+    run_phase(layout, log_tile, mem, n, fac);
+    return 0;
+}
+
+// exp_diag on a density matrix: phase table from diag, then the phase pass (as the GPU path).
+int emu_dm_exp_diag(int layout, unsigned log_tile, double* rho, uint64_t len, unsigned n, const double* diag,
+                    double t, uint32_t* reads, uint32_t* writes, uint64_t* oob) {
+    if (t == 0.0) return 0;
+    const idx_t d = idx_t(1) << n;
+    std::vector<double2> tab(d);
+    for (idx_t x = 0; x < d; ++x) {
+        double sn, cs;
+        sincos(diag[x] * t, &sn, &cs);
+        tab[x] = c2(cs, sn);
+    }
+    TableFactor<EmuMemC2> fac{EmuMemC2{tab.data(), d, oob}};
+    EmuMem mem{reinterpret_cast<double2*>(rho), len, reads, writes, oob};
+    run_phase(layout, log_tile, mem, n, fac);
+    return 0;
+}
+
+int emu_pure_gate1(double* psi, unsigned n, unsigned target, int op, double c, double s, uint32_t* reads,
+                   uint32_t* writes, uint64_t* oob) {
+    if (n < 1 || target >= n) return -1;
+    const idx_t npairs = idx_t(1) << (n - 1);
+    const unsigned grid = grid_for(kPureThreads * kVec, npairs, kSms * 8u);
+    const idx_t nthr = (idx_t)grid * kPureThreads;
+    EmuMem mem{reinterpret_cast<double2*>(psi), idx_t(1) << n, reads, writes, oob};
+    for (idx_t tid = 0; tid < nthr; ++tid) {
+        switch (op) {
+#define ORKAN_EMU_CASE(OPC) case OPC: pure1q_thread<OPC>(mem, npairs, target, c, s, tid, nthr); break;
+            ORKAN_EMU_CASE(kOpX) ORKAN_EMU_CASE(kOpY) ORKAN_EMU_CASE(kOpZ) ORKAN_EMU_CASE(kOpH)
+            ORKAN_EMU_CASE(kOpS) ORKAN_EMU_CASE(kOpSdg) ORKAN_EMU_CASE(kOpT) ORKAN_EMU_CASE(kOpTdg)
+            ORKAN_EMU_CASE(kOpHy) ORKAN_EMU_CASE(kOpRx) ORKAN_EMU_CASE(kOpRy) ORKAN_EMU_CASE(kOpRz)
+            ORKAN_EMU_CASE(kOpP)
+#undef ORKAN_EMU_CASE
+            default: return -1;
+        }
+    }
+    return 0;
+}
+
+int emu_pure_gate2(double* psi, unsigned n, unsigned qa, unsigned qb, int op, uint32_t* reads, uint32_t* writes,
+                   uint64_t* oob) {
+    if (n < 2 || qa >= n || qb >= n || qa == qb) return -1;
+    const idx_t nq = idx_t(1) << (n - 2);
+    const unsigned grid = grid_for(kPureThreads * kVec, nq, kSms * 8u);
+    const idx_t nthr = (idx_t)grid * kPureThreads;
+    EmuMem mem{reinterpret_cast<double2*>(psi), idx_t(1) << n, reads, writes, oob};
+    for (idx_t tid = 0; tid < nthr; ++tid) {
+        switch (op) {
+            case kOpCX: pure2q_thread<kOpCX>(mem, nq, qa, qb, tid, nthr); break;
+            case kOpCY: pure2q_thread<kOpCY>(mem, nq, qa, qb, tid, nthr); break;
+            case kOpCZ: pure2q_thread<kOpCZ>(mem, nq, qa, qb, tid, nthr); break;
+            case kOpSwap: pure2q_thread<kOpSwap>(mem, nq, qa, qb, tid, nthr); break;
+            default: return -1;
+        }
+    }
+    return 0;
+}
+
+int emu_pure_ccx(double* psi, unsigned n, unsigned c1, unsigned c2q, unsigned t, uint32_t* reads, uint32_t* writes,
+                 uint64_t* oob) {
+    if (n < 3) return -1;
+    const idx_t no = idx_t(1) << (n - 3);
+    const unsigned grid = grid_for(kPureThreads * kVec, no, kSms * 8u);
+    const idx_t nthr = (idx_t)grid * kPureThreads;
+    EmuMem mem{reinterpret_cast<double2*>(psi), idx_t(1) << n, reads, writes, oob};
+    for (idx_t tid = 0; tid < nthr; ++tid) pure_ccx_thread(mem, no, c1, c2q, t, tid, nthr);
+    return 0;
+}
+
+int emu_pure_exp_diag(double* psi, unsigned n, const double* diag, double t, uint32_t* reads, uint32_t* writes,
+                      uint64_t* oob) {
+    const idx_t d = idx_t(1) << n;
+    const unsigned grid = grid_for(kPureThreads * kVec, d, kSms * 8u);
+    const idx_t nthr = (idx_t)grid * kPureThreads;
+    EmuMem mem{reinterpret_cast<double2*>(psi), d, reads, writes, oob};
+    EmuMemR dg{diag, d, oob};
+    for (idx_t tid = 0; tid < nthr; ++tid) pure_exp_diag_thread(mem, dg, d, t, tid, nthr);
+    return 0;
+}
+
+int emu_fill(double* data, uint64_t len, double re, double im, unsigned corner_log_tile, uint64_t corner_dim,
+             uint32_t* reads, uint32_t* writes, uint64_t* oob) {
+    const unsigned grid = grid_for(kPureThreads * 4, len, kSms * 8u);
+    const idx_t nthr = (idx_t)grid * kPureThreads;
+    EmuMem mem{reinterpret_cast<double2*>(data), len, reads, writes, oob};
+    for (idx_t tid = 0; tid < nthr; ++tid) fill_thread(mem, len, c2(re, im), corner_log_tile, corner_dim, tid, nthr);
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,175 @@
+"""Python side of the CPU kernel emulator (tests/emu/libkemu.so) -- test infrastructure.
+
+Maps each gate to the kernel-layer operation the host C layer uses for it
+(orkan_b200/csrc/host/gate.c), runs the emulated launch and returns the new storage with
+per-element read/write counts and the number of out-of-range accesses.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "emu", "libkemu.so")
+R2 = 0.70710678118654752440
+LAYOUT = {"pure": 0, "packed": 1, "tiled": 2}
+
+
+def build() -> str:
+    src = os.path.join(HERE, "emu", "emu.cpp")
+    deps = [src] + [os.path.join(HERE, "..", "orkan_b200", "csrc", "cuda", f)
+                    for f in ("common.cuh", "dm_engine.cuh", "dm_phase.cuh", "pure.cuh")]
+    if not os.path.exists(LIB) or any(os.path.getmtime(d) > os.path.getmtime(LIB) for d in deps):
+        import subprocess
+        cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I" + os.path.join(cuda, "include"),
+                        src, "-o", LIB], check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(build())
+    return _lib
+
+
+def _u32(n):
+    return np.zeros(n, dtype=np.uint32)
+
+
+def _arr(x, dt):
+    return np.ascontiguousarray(x, dtype=dt)
+
+
+class Result:
+    def __init__(self, out, reads, writes, oob):
+        self.out, self.reads, self.writes, self.oob = out, reads, writes, oob
+
+
+def _run(fn, data, make_args):
+    out = np.array(data, dtype=np.complex128, copy=True)
+    reads, writes = _u32(out.size), _u32(out.size)
+    oob = C.c_uint64(0)
+    rc = fn(*make_args(out, reads, writes, oob))
+    if rc != 0:
+        raise RuntimeError("emulated launch rejected its parameters")
+    return Result(out, reads, writes, oob.value)
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+# kernel-layer ops -------------------------------------------------------------------
+def dm_unitary(layout, lt, data, n, qubits, u):
+    q = _arr(qubits, np.uint32)
+    uu = _arr(np.asarray(u, dtype=np.complex128).reshape(-1), np.complex128)
+    f = lib().emu_dm_unitary
+    return _run(f, data, lambda o, r, w, b: (LAYOUT[layout], lt, _ptr(o), C.c_uint64(o.size), n, len(q), _ptr(q),
+                                             _ptr(uu), _ptr(r), _ptr(w), C.byref(b)))
+
+
+def dm_monomial(layout, lt, data, n, qubits, src, phase):
+    q = _arr(qubits, np.uint32)
+    s = _arr(src, np.uint32)
+    ph = _arr(phase, np.complex128)
+    f = lib().emu_dm_monomial
+    return _run(f, data, lambda o, r, w, b: (LAYOUT[layout], lt, _ptr(o), C.c_uint64(o.size), n, len(q), _ptr(q),
+                                             _ptr(s), _ptr(ph), _ptr(r), _ptr(w), C.byref(b)))
+
+
+def dm_phase(layout, lt, data, n, qubits, phase):
+    q = _arr(qubits, np.uint32)
+    ph = _arr(phase, np.complex128)
+    f = lib().emu_dm_phase
+    return _run(f, data, lambda o, r, w, b: (LAYOUT[layout], lt, _ptr(o), C.c_uint64(o.size), n, len(q), _ptr(q),
+                                             _ptr(ph), _ptr(r), _ptr(w), C.byref(b)))
+
+
+def dm_superop1(layout, lt, data, n, target, sop):
+    s = _arr(np.asarray(sop).reshape(-1), np.complex128)
+    f = lib().emu_dm_superop1
+    return _run(f, data, lambda o, r, w, b: (LAYOUT[layout], lt, _ptr(o), C.c_uint64(o.size), n, target, _ptr(s),
+                                             _ptr(r), _ptr(w), C.byref(b)))
+
+
+def dm_exp_diag(layout, lt, data, n, diag, t):
+    dg = _arr(diag, np.float64)
+    f = lib().emu_dm_exp_diag
+    f.argtypes = None
+    return _run(f, data, lambda o, r, w, b: (LAYOUT[layout], lt, _ptr(o), C.c_uint64(o.size), n, _ptr(dg),
+                                             C.c_double(t), _ptr(r), _ptr(w), C.byref(b)))
+
+
+PURE_OP1 = {g: i for i, g in enumerate(("x", "y", "z", "h", "s", "sdg", "t", "tdg", "hy", "rx", "ry", "rz", "p"))}
+PURE_OP2 = {"cx": 0, "cy": 1, "cz": 2, "swap": 3}
+
+
+def pure_gate(data, n, name, qubits, theta=None):
+    lb = lib()
+    if name in PURE_OP1:
+        c = s = 0.0
+        if name in ("rx", "ry", "rz"):
+            c, s = np.cos(theta / 2.0), np.sin(theta / 2.0)
+        elif name == "p":
+            c, s = np.cos(theta), np.sin(theta)
+        return _run(lb.emu_pure_gate1, data, lambda o, r, w, b: (_ptr(o), n, int(qubits[0]), PURE_OP1[name],
+                                                                   C.c_double(c), C.c_double(s), _ptr(r), _ptr(w),
+                                                                   C.byref(b)))
+    if name in PURE_OP2:
+        return _run(lb.emu_pure_gate2, data, lambda o, r, w, b: (_ptr(o), n, int(qubits[0]), int(qubits[1]),
+                                                                   PURE_OP2[name], _ptr(r), _ptr(w), C.byref(b)))
+    return _run(lb.emu_pure_ccx, data, lambda o, r, w, b: (_ptr(o), n, int(qubits[0]), int(qubits[1]),
+                                                            int(qubits[2]), _ptr(r), _ptr(w), C.byref(b)))
+
+
+def pure_exp_diag(data, n, diag, t):
+    dg = _arr(diag, np.float64)
+    return _run(lib().emu_pure_exp_diag, data, lambda o, r, w, b: (_ptr(o), n, _ptr(dg), C.c_double(t), _ptr(r),
+                                                                     _ptr(w), C.byref(b)))
+
+
+def fill(length, value, corner_log_tile=0, corner_dim=0):
+    data = np.zeros(length, dtype=np.complex128)
+    return _run(lib().emu_fill, data, lambda o, r, w, b: (_ptr(o), C.c_uint64(length), C.c_double(value.real),
+                                                           C.c_double(value.imag), corner_log_tile,
+                                                           C.c_uint64(corner_dim), _ptr(r), _ptr(w), C.byref(b)))
+
+
+def dm_gate(layout, lt, data, n, name, qubits, theta=None):
+    """The kernel-layer call the host C layer makes for this gate (gate.c)."""
+    q = list(qubits)
+    if name == "x":
+        return dm_monomial(layout, lt, data, n, q, [1, 0], [1, 1])
+    if name == "y":
+        return dm_monomial(layout, lt, data, n, q, [1, 0], [-1j, 1j])
+    if name in ("z", "s", "sdg", "t", "tdg", "p", "rz"):
+        ph1 = {"z": -1, "s": 1j, "sdg": -1j, "t": R2 + 1j * R2, "tdg": R2 - 1j * R2}.get(name)
+        if ph1 is None:
+            ph1 = np.cos(theta) + 1j * np.sin(theta)
+        return dm_phase(layout, lt, data, n, q, [1, ph1])
+    if name == "h":
+        return dm_unitary(layout, lt, data, n, q, [[R2, R2], [R2, -R2]])
+    if name == "hy":
+        return dm_unitary(layout, lt, data, n, q, [[R2, -R2], [R2, R2]])
+    if name in ("rx", "ry"):
+        c, s = np.cos(theta / 2.0), np.sin(theta / 2.0)
+        u = [[c, -1j * s], [-1j * s, c]] if name == "rx" else [[c, -s], [s, c]]
+        return dm_unitary(layout, lt, data, n, q, u)
+    if name == "cx":
+        return dm_monomial(layout, lt, data, n, q, [0, 1, 3, 2], [1, 1, 1, 1])
+    if name == "cy":
+        return dm_monomial(layout, lt, data, n, q, [0, 1, 3, 2], [1, 1, -1j, 1j])
+    if name == "cz":
+        return dm_phase(layout, lt, data, n, q, [1, 1, 1, -1])
+    if name == "swap":
+        return dm_monomial(layout, lt, data, n, q, [0, 2, 1, 3], [1, 1, 1, 1])
+    if name == "ccx":
+        return dm_monomial(layout, lt, data, n, q, [0, 1, 2, 3, 4, 5, 7, 6], [1] * 8)
+    raise ValueError(name)
