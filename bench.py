@@ -1,0 +1,436 @@
+#!/usr/bin/env python
+"""Single-gate throughput sweep of the Orkan state-update path on B200.
+
+Workload (one "step"): the sweep of orkan_b200/workloads.sweep() -- every 1-qubit gate on
+every target, CX/CY/CZ/SWAP on (low, high), (high, low) and adjacent pairs, CCX on spread
+and adjacent triples -- applied to a 30-qubit PURE statevector (16 GiB, Gaussian random,
+normalised) and to 14-qubit density matrices in the tiled and the packed layout
+(Dirichlet(1,1,1,1) mixtures of 4 Gaussian pure states, 2.15 GB each).  Rotation angles
+are uniform in [0, 2 pi).  Inputs are larger than the 126 MB L2, so no flush is needed.
+
+Metric: GB/s of algorithmic bytes (orkan_b200/traffic.py: 2 x 32 B x sectors that hold an
+element the gate may change) over device time.  `value` times the sweep on resident
+states with CUDA events; `e2e` repeats it through the public C API from pinned host
+buffers (state upload, sweep, mean() of a [-1, 1] observable passed as a host pointer,
+result read back), copies inside the timed region.
+
+  python bench.py [--gpus N --steps K --warmup W]            # this library on N GPUs
+  python bench.py --impl reference [...]                     # the reference CPU library
+Multi-GPU: replicas (each rank runs the whole workload on its GPU; no collective on the
+data path); value = all ranks' bytes / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "gate/channel GB/s (single-gate throughput sweep)"
+UNIT = "GB/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["orkan", "reference"], default="orkan")
+    ap.add_argument("--pure-qubits", type=int, default=30)
+    ap.add_argument("--mixed-qubits", type=int, default=14)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def kernel_class(kind: str, name: str) -> str:
+    from orkan_b200 import traffic as T
+    if kind == "pure":
+        if name in ("cx", "cy", "cz", "swap"):
+            return "pure_2q"
+        if name == "ccx":
+            return "pure_ccx"
+        return "pure_1q_dense" if (name in T.DENSE_1Q or name == "rz") else "pure_1q_phase"
+    if name in T.PHASE_1Q or name == "cz":
+        return f"{kind}_phase"
+    return f"{kind}_engine"
+
+
+def build_plan(npure: int, nmix: int, log_tile: int = 5):
+    """[(kind, n, name, qubits, theta, bytes, class)] for one step."""
+    from orkan_b200 import traffic as T
+    from orkan_b200 import workloads as W
+    plan = []
+    for kind, n in (("pure", npure), ("tiled", nmix), ("packed", nmix)):
+        for name, qs, th in W.sweep(n):
+            plan.append((kind, n, name, qs, th, T.gate_bytes(kind, n, name, qs, log_tile), kernel_class(kind, name)))
+    return plan
+
+
+# ---------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if not self.proc:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=10)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return out
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        out["samples"] = len(rows)
+        out["sm_mhz"] = sm[len(sm) // 2] if sm else None
+        try:
+            out["sm_max_mhz"] = float(rows[0][2])
+        except ValueError:
+            pass
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = set()
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        out["reasons"] = sorted(reasons)
+        try:
+            out["power_w_max"] = max(float(r[3]) for r in rows)
+        except ValueError:
+            pass
+        return out
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per launch of each kernel class from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ---------------------------------------------------------------------------------------
+# CPU reference (the reference library compiled from its own sources, oracle/_ref)
+# ---------------------------------------------------------------------------------------
+def reference_lib(threads: int):
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
+    from oracle import ref
+    if not ref.available(5):
+        return None
+    return ref.RefLib(5)
+
+
+def reference_states(lib, npure, nmix, seed=1):
+    from orkan_b200 import workloads as W
+    states = {}
+    for kind, n in (("pure", npure), ("tiled", nmix), ("packed", nmix)):
+        storage = W.initial_storage(kind, n, seed, log_tile=5)
+        states[kind] = lib.state(kind, n, storage)
+        del storage
+    return states
+
+
+def time_reference_sample(lib, states, plan, stride, offset):
+    """Run every stride-th plan entry (starting at offset); return (bytes, seconds)."""
+    nbytes, secs = 0, 0.0
+    for i, (kind, n, name, qs, th, b, _) in enumerate(plan):
+        if i % stride != offset % stride:
+            continue
+        t0 = time.perf_counter()
+        lib.gate(states[kind], name, qs, th)
+        secs += time.perf_counter() - t0
+        nbytes += b
+    return nbytes, secs
+
+
+def cpu_baseline(plan, npure, nmix, budget_s):
+    cores = host_cores()
+    lib = reference_lib(cores)
+    if lib is None:
+        return None
+    states = reference_states(lib, npure, nmix)
+    # warm the pages, then time a strided sample sized to the budget
+    first = [(i, e) for i, e in enumerate(plan)]
+    t0 = time.perf_counter()
+    lib.gate(states["pure"], "h", (0,))
+    est = max(time.perf_counter() - t0, 1e-3)
+    stride = max(1, int(math.ceil(len(plan) * est / budget_s)))
+    nbytes, secs = time_reference_sample(lib, states, plan, stride, 0)
+    for s in states.values():
+        lib.free(s)
+    return {"value": nbytes / secs / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"every {stride}th gate of the sweep ({len(first[::stride])} gates, {secs:.1f} s) on the same "
+                      f"{npure} q PURE / {nmix} q tiled / {nmix} q packed states, OpenMP threads = {cores}"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    plan = build_plan(args.pure_qubits, args.mixed_qubits)
+    cores = host_cores()
+    lib = reference_lib(cores)
+    config = {"workload": f"single-gate throughput sweep: {args.pure_qubits} q PURE, {args.mixed_qubits} q tiled "
+                          f"and packed density matrices, {len(plan)} gate applications per full sweep",
+              "pure_qubits": args.pure_qubits, "mixed_qubits": args.mixed_qubits, "sample": "strided"}
+    if lib is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/liborkan_ref_t5.so not built"}))
+        return 0
+    states = reference_states(lib, args.pure_qubits, args.mixed_qubits)
+    t0 = time.perf_counter()
+    lib.gate(states["pure"], "h", (0,))
+    est = max(time.perf_counter() - t0, 1e-3)
+    stride = max(1, int(math.ceil(len(plan) * est / 8.0)))     # about 8 s of gate work per step
+    for w in range(args.warmup):
+        time_reference_sample(lib, states, plan, stride, w)
+    tot_b, tot_s = 0, 0.0
+    for k in range(args.steps):
+        b, s = time_reference_sample(lib, states, plan, stride, args.warmup + k)
+        tot_b += b
+        tot_s += s
+    value = tot_b / tot_s / 1e9
+    sample = (f"every {stride}th gate of the sweep per step ({args.steps} steps, {tot_s:.1f} s of gate time), "
+              f"OpenMP threads = {cores}")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian states, uniform angles)", "config": config,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------------------
+# this library on the GPU
+# ---------------------------------------------------------------------------------------
+def run_gpu(args):
+    import numpy as np
+    import torch
+
+    import orkan_b200
+    from orkan_b200 import workloads as W
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ork = orkan_b200.load(5)
+    ork.set_stream(torch.cuda.current_stream().cuda_stream)
+    plan = build_plan(args.pure_qubits, args.mixed_qubits)
+    step_bytes = sum(e[5] for e in plan)
+
+    # states (generated on the device, seeded) and observables
+    states, host_in, obs_dev, obs_host, nbytes_state = {}, {}, {}, {}, {}
+    pinned = True
+    for kind, n in (("pure", args.pure_qubits), ("tiled", args.mixed_qubits), ("packed", args.mixed_qubits)):
+        st = ork.state(kind, n)
+        W.fill_state_on_device(ork, st, kind, n, seed=1 + rank, log_tile=5)
+        states[kind] = st
+        obs = W.uniform_obs_torch(n, seed=7)
+        obs_dev[kind] = obs
+        nbytes_state[kind] = int(ork.lib.state_len(orkan_b200.C.byref(st))) * 16
+        if not args.no_e2e:
+            try:
+                h = torch.empty(nbytes_state[kind] // 16, dtype=torch.complex128, pin_memory=pinned)
+                o = torch.empty(1 << n, dtype=torch.float64, pin_memory=pinned)
+            except RuntimeError:
+                pinned = False
+                h = torch.empty(nbytes_state[kind] // 16, dtype=torch.complex128)
+                o = torch.empty(1 << n, dtype=torch.float64)
+            h.copy_(W.state_view(ork, st))
+            o.copy_(obs)
+            host_in[kind], obs_host[kind] = h, o
+    torch.cuda.synchronize()
+
+    def sweep(record=None):
+        for i, (kind, n, name, qs, th, b, cls) in enumerate(plan):
+            ork.gate(states[kind], name, qs, th)
+            if record is not None:
+                record[i].record()
+
+    for _ in range(args.warmup):
+        sweep()
+    torch.cuda.synchronize()
+
+    # ---- device-timed region ----
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in plan] for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = ork.launches()
+    start.record()
+    for k in range(args.steps):
+        sweep(ev[k])
+    end.record()
+    torch.cuda.synchronize()
+    launches = ork.launches() - launches0
+    barrier()
+    clk = clocks.stop()
+    total_ms = start.elapsed_time(end)
+    per_class_ms, per_class_bytes, per_class_n = {}, {}, {}
+    for k in range(args.steps):
+        prev = start if k == 0 else ev[k - 1][-1]
+        for i, e in enumerate(plan):
+            dt = prev.elapsed_time(ev[k][i])
+            prev = ev[k][i]
+            cls = e[6]
+            per_class_ms[cls] = per_class_ms.get(cls, 0.0) + dt
+            per_class_bytes[cls] = per_class_bytes.get(cls, 0) + e[5]
+            per_class_n[cls] = per_class_n.get(cls, 0) + 1
+    max_ms = max_over_ranks(total_ms)
+    value = world * args.steps * step_bytes / (max_ms * 1e-3) / 1e9
+
+    # ---- end to end through the public API with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        for kind in states:                        # untimed: same code path once
+            ork.upload(states[kind], host_in[kind].numpy())
+        barrier()
+        torch.cuda.synchronize()
+        e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        results = []
+        e_start.record()
+        for k in range(args.steps):
+            for kind in states:
+                rc = ork.lib.orkan_state_upload(orkan_b200.C.byref(states[kind]), host_in[kind].data_ptr())
+                if rc:
+                    raise RuntimeError(f"upload failed ({rc})")
+            sweep()
+            for kind in states:
+                results.append(ork.mean(states[kind], obs_host[kind].data_ptr()))
+        e_end.record()
+        torch.cuda.synchronize()
+        barrier()
+        e_ms = max_over_ranks(e_start.elapsed_time(e_end))
+        h2d = sum(nbytes_state.values()) + sum(8 * (1 << n) for n in (args.pure_qubits, args.mixed_qubits,
+                                                                          args.mixed_qubits))
+        e2e = {"value": world * args.steps * step_bytes / (e_ms * 1e-3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * len(states), "ms_per_step": e_ms / args.steps,
+               "pinned_host_buffers": pinned, "means": [float(x) for x in results[-3:]]}
+
+    # ---- roofline of the dominant kernel ----
+    dom = max(per_class_ms, key=per_class_ms.get)
+    peak, peak_kind = measured_peak()
+    launches_dom = per_class_n[dom]
+    avg_ms = per_class_ms[dom] / launches_dom
+    avg_bytes = per_class_bytes[dom] / launches_dom
+    achieved = avg_bytes / (avg_ms * 1e-3) / 1e9
+    traffic = profiled_traffic().get(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "algorithmic_bytes_per_launch": avg_bytes, "avg_launch_ms": avg_ms, "launches": launches_dom}
+    classes = {c: {"launches": per_class_n[c], "ms": per_class_ms[c], "share": per_class_ms[c] / sum(per_class_ms.values()),
+                   "GB/s": per_class_bytes[c] / (per_class_ms[c] * 1e-3) / 1e9} for c in sorted(per_class_ms)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # free device memory first is not needed; the CPU baseline runs on host memory
+        cpu = cpu_baseline(plan, args.pure_qubits, args.mixed_qubits, args.cpu_seconds)
+
+    for st in states.values():
+        ork.free(st)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded Gaussian states, Dirichlet mixtures, uniform angles)",
+                "config": {"workload": f"single-gate throughput sweep: {args.pure_qubits} q PURE statevector + "
+                                       f"{args.mixed_qubits} q tiled and packed density matrices, "
+                                       f"{len(plan)} gate applications per step",
+                           "pure_qubits": args.pure_qubits, "mixed_qubits": args.mixed_qubits,
+                           "gates_per_step": len(plan), "algorithmic_bytes_per_step": step_bytes,
+                           "l2": "inputs larger than L2 (16 GiB and 2.15 GB states vs 126 MB L2); no flush",
+                           "parallelism": f"replicas x{world}"},
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+                "gpu_launches": launches, "kernel_classes": classes}
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -85,3 +85,94 @@ def sweep(n: int):
     for tr in triples:
         out.append(("ccx", tr, None))
     return out
+
+
+# ---------------------------------------------------------------------------------------
+# device-side generation of the large benchmark states (torch is only the RNG/plumbing)
+# ---------------------------------------------------------------------------------------
+class _DeviceArray:
+    """Zero-copy view of library-owned device memory for torch (__cuda_array_interface__)."""
+
+    def __init__(self, ptr: int, count: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def state_view(ork, st):
+    """torch complex128 tensor aliasing a state's device storage."""
+    import ctypes as C
+
+    import torch
+    count = int(ork.lib.state_len(C.byref(st)))
+    return torch.as_tensor(_DeviceArray(int(st.data), count, "<c16"), device="cuda")
+
+
+def storage_rc_torch(kind: str, n: int, log_tile: int, device="cuda"):
+    """(row, col, live) of every storage index, on the device."""
+    import torch
+    d = 1 << n
+    if kind == "packed":
+        idx = torch.triu_indices(d, d, device=device)
+        return idx[1], idx[0], None
+    t = 1 << log_tile
+    nt = (d + t - 1) // t
+    e = torch.arange(nt * (nt + 1) // 2 * t * t, device=device, dtype=torch.int64)
+    tile = e >> (2 * log_tile)
+    lr = (e >> log_tile) & (t - 1)
+    lc = e & (t - 1)
+    tr = torch.floor((torch.sqrt(8.0 * tile.double() + 1.0) - 1.0) / 2).long()
+    tr = torch.where(tr * (tr + 1) // 2 > tile, tr - 1, tr)
+    tr = torch.where((tr + 1) * (tr + 2) // 2 <= tile, tr + 1, tr)
+    tc = tile - tr * (tr + 1) // 2
+    r, c = tr * t + lr, tc * t + lc
+    return r, c, (r < d) & (c < d)
+
+
+def initial_storage_torch(kind: str, n: int, seed: int, log_tile: int = 5, device="cuda"):
+    """Storage of the benchmark's initial state: a Gaussian normalised statevector, or a
+    Dirichlet(1,1,1,1) mixture of 4 Gaussian normalised states in the given layout."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    d = 1 << n
+
+    def gauss():
+        v = torch.complex(torch.randn(d, generator=g, device=device, dtype=torch.float64),
+                          torch.randn(d, generator=g, device=device, dtype=torch.float64))
+        return v / torch.linalg.vector_norm(v)
+
+    if kind == "pure":
+        return gauss()
+    w = np.random.default_rng(seed).dirichlet(np.ones(4))
+    r, c, live = storage_rc_torch(kind, n, log_tile, device)
+    out = torch.zeros(r.shape[0], dtype=torch.complex128, device=device)
+    for wi in w:
+        p = gauss()
+        term = p[r.clamp(max=d - 1)] * torch.conj(p[c.clamp(max=d - 1)])
+        out += float(wi) * (term if live is None else torch.where(live, term, torch.zeros_like(term)))
+        del term, p
+    return out
+
+
+def initial_storage(kind: str, n: int, seed: int, log_tile: int = 5) -> np.ndarray:
+    """Host copy of initial_storage_torch (generated on the GPU when one is present)."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return initial_storage_torch(kind, n, seed, log_tile).cpu().numpy()
+        return initial_storage_torch(kind, n, seed, log_tile, device="cpu").numpy()
+    except ImportError:
+        raise RuntimeError("torch is needed to generate the benchmark states")
+
+
+def fill_state_on_device(ork, st, kind: str, n: int, seed: int, log_tile: int = 5) -> None:
+    import torch
+    state_view(ork, st).copy_(initial_storage_torch(kind, n, seed, log_tile))
+    torch.cuda.synchronize()
+
+
+def uniform_obs_torch(n: int, seed: int):
+    import torch
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    return torch.rand(1 << n, generator=g, device="cuda", dtype=torch.float64) * 2.0 - 1.0
