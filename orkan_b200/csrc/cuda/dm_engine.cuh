@@ -46,6 +46,9 @@ struct DmGeom {
     unsigned vbit[3];   // virtual-index bit of gate qubit j; j = 0 is the MSB of the local index
     idx_t nbase;        // base segments per dimension: (d >> ls) >> h
     idx_t items;        // nbase * (nbase + 1) / 2
+    unsigned fixmask;   // bit l set: local index l is left in place with phase 1 by the gate
+                        // (monomial gates only; an element whose row and column are both
+                        // fixed is unchanged and is neither loaded nor stored)
     ORKAN_HD unsigned S() const { return 1u << ls; }
     ORKAN_HD unsigned V() const { return 1u << (ls + h); }
     ORKAN_HD unsigned P() const { return V() + 1; }    // smem row pitch (padded)
@@ -88,6 +91,7 @@ inline bool dm_geometry(unsigned n, unsigned k, const unsigned* qubits, unsigned
             for (unsigned j = k; j < 3; ++j) g->vbit[j] = 0;
             g->nbase = (g->d >> ls) >> h;
             g->items = g->nbase * (g->nbase + 1) / 2;
+            g->fixmask = 0;
             return true;
         }
         if (ls == 0) return false;
@@ -132,41 +136,67 @@ ORKAN_HD void dm_line_pos(unsigned e, unsigned ls, unsigned* i, unsigned* j) {
     if (Map::kRowContig) { *i = pos; *j = line; } else { *i = line; *j = pos; }
 }
 
-// Stage one item into the shared block vb (pitch P).
+ORKAN_HD unsigned dm_get_local(unsigned x, const unsigned* vbit, unsigned k);
+
+// Is the element at virtual (vr, vc) unchanged by the gate (row and column fixed)?
+ORKAN_HD bool dm_fixed(const DmGeom& g, unsigned vr, unsigned vc) {
+    if (!g.fixmask) return false;
+    return ((g.fixmask >> dm_get_local(vr, g.vbit, g.k)) & (g.fixmask >> dm_get_local(vc, g.vbit, g.k)) & 1u) != 0;
+}
+
+// Stage one item into the shared block vb (pitch P).  Each thread first issues all of
+// its global loads (up to kDmMaxElems / kDmThreads = 16, so a block keeps its whole 64 KB
+// item in flight), then writes them to shared memory.
+constexpr unsigned kDmEpt = kDmMaxElems / kDmThreads;
+constexpr unsigned kNoSlot = 0xffffffffu;
+
 template <class Map, class Mem>
 ORKAN_HD void dm_load(const Mem& mem, const Map& map, const DmGeom& g, const DmItem& it,
                       double2* vb, unsigned tid, unsigned nthr) {
     const unsigned S = g.S(), P = g.P(), ls = g.ls, h = g.h;
     const unsigned total = 1u << (2 * (ls + h));
-    for (unsigned f = tid; f < total; f += nthr) {
-        const unsigned pos = f >> (2 * ls), e = f & ((1u << (2 * ls)) - 1);
-        const unsigned a = pos >> h, b = pos & ((1u << h) - 1);
-        unsigned i, j;
-        dm_line_pos<Map>(e, ls, &i, &j);
-        const idx_t R = it.rseg[a], C = it.cseg[b];
-        switch (dm_sub_class(it, a, b)) {
-            case kSubDirect: {
-                const double2 v = mem.ld(map.at(R + i, C + j));
-                vb[(a * S + i) * P + b * S + j] = v;
-                if (it.diag) vb[(b * S + j) * P + a * S + i] = cconj(v);
-                break;
+    for (unsigned f0 = tid; f0 < total; f0 += nthr * kDmEpt) {
+        double2 v[kDmEpt];
+        unsigned dst[kDmEpt], dstc[kDmEpt];   // direct / conjugated destination (kNoSlot = none)
+#pragma unroll
+        for (unsigned u = 0; u < kDmEpt; ++u) {
+            const unsigned f = f0 + u * nthr;
+            dst[u] = kNoSlot;
+            dstc[u] = kNoSlot;
+            if (f >= total) continue;
+            const unsigned pos = f >> (2 * ls), e = f & ((1u << (2 * ls)) - 1);
+            const unsigned a = pos >> h, b = pos & ((1u << h) - 1);
+            unsigned i, j;
+            dm_line_pos<Map>(e, ls, &i, &j);
+            const idx_t R = it.rseg[a], C = it.cseg[b];
+            switch (dm_sub_class(it, a, b)) {
+                case kSubDirect:
+                    if (dm_fixed(g, a * S + i, b * S + j)) break;
+                    v[u] = mem.ld(map.at(R + i, C + j));
+                    dst[u] = (a * S + i) * P + b * S + j;
+                    if (it.diag) dstc[u] = (b * S + j) * P + a * S + i;
+                    break;
+                case kSubDiag:
+                    if (i >= j && !dm_fixed(g, a * S + i, a * S + j)) {
+                        v[u] = mem.ld(map.at(R + i, R + j));
+                        dst[u] = (a * S + i) * P + a * S + j;
+                        if (i > j) dstc[u] = (a * S + j) * P + a * S + i;
+                    }
+                    break;
+                case kSubTransposed:
+                    // stored partner (C, R): its element (i, j) is virtual (R + j, C + i), conjugated
+                    if (dm_fixed(g, a * S + j, b * S + i)) break;
+                    v[u] = mem.ld(map.at(C + i, R + j));
+                    dstc[u] = (a * S + j) * P + b * S + i;
+                    break;
+                default:
+                    break;
             }
-            case kSubDiag: {
-                if (i >= j) {
-                    const double2 v = mem.ld(map.at(R + i, R + j));
-                    vb[(a * S + i) * P + a * S + j] = v;
-                    if (i > j) vb[(a * S + j) * P + a * S + i] = cconj(v);
-                }
-                break;
-            }
-            case kSubTransposed: {
-                // stored partner (C, R): its element (i, j) is virtual (R + j, C + i), conjugated
-                const double2 v = mem.ld(map.at(C + i, R + j));
-                vb[(a * S + j) * P + b * S + i] = cconj(v);
-                break;
-            }
-            default:
-                break;
+        }
+#pragma unroll
+        for (unsigned u = 0; u < kDmEpt; ++u) {
+            if (dst[u] != kNoSlot) vb[dst[u]] = v[u];
+            if (dstc[u] != kNoSlot) vb[dstc[u]] = cconj(v[u]);
         }
     }
 }
@@ -185,12 +215,14 @@ ORKAN_HD void dm_store(const Mem& mem, const Map& map, const DmGeom& g, const Dm
         const idx_t R = it.rseg[a], C = it.cseg[b];
         switch (dm_sub_class(it, a, b)) {
             case kSubDirect: {
+                if (dm_fixed(g, a * S + i, b * S + j)) break;
                 const double2 v = vb[(a * S + i) * P + b * S + j];
                 mem.st(map.at(R + i, C + j), v);
                 if (Map::kMirrors && map.same_storage_block(R, C)) mem.st(map.at(C + j, R + i), cconj(v));
                 break;
             }
             case kSubDiag: {
+                if (dm_fixed(g, a * S + i, a * S + j)) break;
                 if (i >= j) {
                     mem.st(map.at(R + i, R + j), vb[(a * S + i) * P + a * S + j]);
                 } else if (Map::kMirrors) {
@@ -199,6 +231,7 @@ ORKAN_HD void dm_store(const Mem& mem, const Map& map, const DmGeom& g, const Dm
                 break;
             }
             case kSubTransposed: {
+                if (dm_fixed(g, a * S + j, b * S + i)) break;
                 const double2 v = vb[(a * S + j) * P + b * S + i];
                 mem.st(map.at(C + i, R + j), cconj(v));
                 if (Map::kMirrors && map.same_storage_block(C, R)) mem.st(map.at(R + j, C + i), v);
@@ -336,6 +369,14 @@ struct OpMonomial {
         }
     }
 };
+
+// Local indices the monomial gate leaves in place with phase exactly 1.
+inline unsigned monomial_fixmask(const OpMonomial& op, unsigned m) {
+    unsigned mask = 0;
+    for (unsigned l = 0; l < m; ++l)
+        if (op.src[l] == l && op.phase[l].x == 1.0 && op.phase[l].y == 0.0) mask |= 1u << l;
+    return mask;
+}
 
 // Kernel body for one work item, split into phases separated by block barriers.
 template <class Map, class Mem, class Op>

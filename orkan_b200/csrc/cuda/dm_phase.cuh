@@ -72,6 +72,8 @@ ORKAN_HD double2 phase_apply(double2 f, double2 v) {
     return c2(f.x * v.x - f.y * v.y, f.x * v.y + f.y * v.x);
 }
 
+constexpr unsigned kPhaseEpt = 4;   // elements per thread per trip: loads issued together
+
 template <class Map, class Mem, class Factor>
 ORKAN_HD void dm_phase_item(const Mem& mem, const Map& map, const PhaseGeom& g, const Factor& fac,
                             idx_t w, unsigned tid, unsigned nthr) {
@@ -82,17 +84,32 @@ ORKAN_HD void dm_phase_item(const Mem& mem, const Map& map, const PhaseGeom& g, 
     const unsigned total = S * S;
     const bool diag = (u == v);
     const bool mirror = Map::kMirrors && !diag && map.same_storage_block(R, C);
-    for (unsigned e = tid; e < total; e += nthr) {
-        const unsigned line = e >> ls, pos = e & (S - 1);
-        unsigned i, j;
-        if (Map::kRowContig) { i = pos; j = line; } else { i = line; j = pos; }
-        if (diag && i <= j) continue;
-        double2 f;
-        if (!fac.factor(R + i, C + j, &f)) continue;
-        const idx_t a = map.at(R + i, C + j);
-        const double2 nv = phase_apply(f, mem.ld(a));
-        mem.st(a, nv);
-        if (Map::kMirrors && (diag || mirror)) mem.st(map.at(C + j, R + i), cconj(nv));
+    for (unsigned e0 = tid; e0 < total; e0 += nthr * kPhaseEpt) {
+        idx_t addr[kPhaseEpt], maddr[kPhaseEpt];
+        double2 f[kPhaseEpt], val[kPhaseEpt];
+        bool act[kPhaseEpt];
+#pragma unroll
+        for (unsigned k = 0; k < kPhaseEpt; ++k) {
+            const unsigned e = e0 + k * nthr;
+            act[k] = false;
+            if (e >= total) continue;
+            const unsigned line = e >> ls, pos = e & (S - 1);
+            unsigned i, j;
+            if (Map::kRowContig) { i = pos; j = line; } else { i = line; j = pos; }
+            if (diag && i <= j) continue;
+            if (!fac.factor(R + i, C + j, &f[k])) continue;
+            act[k] = true;
+            addr[k] = map.at(R + i, C + j);
+            maddr[k] = (Map::kMirrors && (diag || mirror)) ? map.at(C + j, R + i) : addr[k];
+            val[k] = mem.ld(addr[k]);
+        }
+#pragma unroll
+        for (unsigned k = 0; k < kPhaseEpt; ++k) {
+            if (!act[k]) continue;
+            const double2 nv = phase_apply(f[k], val[k]);
+            mem.st(addr[k], nv);
+            if (maddr[k] != addr[k]) mem.st(maddr[k], cconj(nv));
+        }
     }
 }
 

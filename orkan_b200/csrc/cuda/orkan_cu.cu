@@ -207,6 +207,7 @@ int orkan_cu_dm_monomial(int layout, unsigned log_tile, void* rho, unsigned n, u
     }
     DmGeom g;
     if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g)) return (int)cudaErrorInvalidValue;
+    g.fixmask = monomial_fixmask(op, m);
     return launch_engine_map(layout, log_tile, rho, n, g, op, as_stream(stream));
 }
 

@@ -138,6 +138,7 @@ int emu_dm_monomial(int layout, unsigned log_tile, double* rho, uint64_t len, un
     for (unsigned y = 0; y < (1u << k); ++y) { op.src[y] = src[y]; op.phase[y] = ldc(phase, y); }
     DmGeom g;
     if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g)) return -1;
+    g.fixmask = monomial_fixmask(op, 1u << k);
     return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
 }
 
