@@ -69,6 +69,7 @@ struct PackedMap {
     static constexpr bool kRowContig = true;   // consecutive rows are adjacent
     static constexpr bool kMirrors = false;    // no stored upper-triangle copies
     ORKAN_HD bool same_storage_block(idx_t, idx_t) const { return false; }
+    ORKAN_HD unsigned log_tdim() const { return 0; }
 };
 
 // MIXED_TILED: lower-triangular grid of 2^L x 2^L tiles, tiles in row-major tile
@@ -90,6 +91,7 @@ struct TiledMap {
     static constexpr bool kMirrors = true;     // diagonal tiles store the upper half too
     // Do rows r and c fall into the same tile row (so (r,c) and (c,r) share a tile)?
     ORKAN_HD bool same_storage_block(idx_t r, idx_t c) const { return (r >> L) == (c >> L); }
+    ORKAN_HD unsigned log_tdim() const { return L; }
 };
 
 // ---------------------------------------------------------------------------------

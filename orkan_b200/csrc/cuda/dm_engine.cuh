@@ -49,6 +49,7 @@ struct DmGeom {
     unsigned fixmask;   // bit l set: local index l is left in place with phase 1 by the gate
                         // (monomial gates only; an element whose row and column are both
                         // fixed is unchanged and is neither loaded nor stored)
+    unsigned long long fixrows;  // the same as a mask over virtual indices (dm_fixed_rows)
     ORKAN_HD unsigned S() const { return 1u << ls; }
     ORKAN_HD unsigned V() const { return 1u << (ls + h); }
     ORKAN_HD unsigned P() const { return V() + 1; }    // smem row pitch (padded)
@@ -92,154 +93,204 @@ inline bool dm_geometry(unsigned n, unsigned k, const unsigned* qubits, unsigned
             g->nbase = (g->d >> ls) >> h;
             g->items = g->nbase * (g->nbase + 1) / 2;
             g->fixmask = 0;
+            g->fixrows = 0;
             return true;
         }
         if (ls == 0) return false;
     }
 }
 
-// Row/column segment origins of one work item.
-struct DmItem {
-    idx_t rseg[8];
-    idx_t cseg[8];
-    bool diag;          // row base == column base
-};
-
-ORKAN_HD void dm_item(const DmGeom& g, idx_t w, DmItem& it) {
-    idx_t u, v;
-    tri_unrank(w, &u, &v);
-    const idx_t rb = insert0_sorted(u, g.hb, g.h);
-    const idx_t cb = insert0_sorted(v, g.hb, g.h);
-    for (unsigned a = 0; a < (1u << g.h); ++a) {
-        const idx_t off = spread_bits(a, g.hb, g.h);
-        it.rseg[a] = (rb | off) << g.ls;
-        it.cseg[a] = (cb | off) << g.ls;
-    }
-    it.diag = (u == v);
-}
-
 // Sub-tile classes of position (a, b) of an item.
 enum : int { kSubDirect = 0, kSubDiag = 1, kSubTransposed = 2, kSubSkip = 3 };
 
-ORKAN_HD int dm_sub_class(const DmItem& it, unsigned a, unsigned b) {
-    const idx_t R = it.rseg[a], C = it.cseg[b];
-    if (R > C) return kSubDirect;
-    if (R == C) return kSubDiag;
-    return it.diag ? kSubSkip : kSubTransposed;
-}
+// Per-position descriptor of an item, built once per item in shared memory so that each
+// element's storage index, shared-memory slot(s) and skip test cost a few integer ops.
+// A "line" is a run of S consecutive storage elements of a stored sub-tile (a column
+// segment of the packed layout, a row segment of a tile); p is the offset along it.
+struct DmPos {
+    idx_t gbase;   // storage index of element (line 0, p 0) of the stored sub-tile
+    idx_t mbase;   // tiled: storage index of the mirror of (line 0, p 0); written at mbase + p*T + line
+    idx_t gcol;    // packed: d - PC - 1, the column-start increment per line
+    int d0, dl, dp;  // direct shared-memory slot: d0 + line*dl + p*dp
+    int c0, cl, cp;  // conjugated shared-memory slot
+    int fconst;      // virtual index constant along a line is fconst + line
+    int fvar;        // virtual index varying along a line is fvar + p
+    int cls;         // kSub*
+    int has_c;       // a direct sub-tile that also fills its transposed position (diagonal item)
+    int mirror;      // tiled: the stored sub-tile lies in a diagonal tile; rewrite its mirror
+    int pad_;
+};
+constexpr unsigned kDmMaxPos = 64;                     // 4^h with h <= 3
+constexpr unsigned kDmPosBytes = kDmMaxPos * sizeof(DmPos);
 
-// Element (i, j) of the stored sub-tile visited by flat index e, so that consecutive
-// e walk the layout's contiguous direction.
-template <class Map>
-ORKAN_HD void dm_line_pos(unsigned e, unsigned ls, unsigned* i, unsigned* j) {
-    const unsigned line = e >> ls, pos = e & ((1u << ls) - 1);
-    if (Map::kRowContig) { *i = pos; *j = line; } else { *i = line; *j = pos; }
-}
+// Shared memory of one block: descriptors, then the V x (V + 1) staged block.
+ORKAN_HD size_t dm_smem_bytes(const DmGeom& g) { return kDmPosBytes + (size_t)g.V() * g.P() * 16; }
 
+// Virtual-index bit masks of fixed rows/columns (monomial gates): bit x set when local(x)
+// is left in place with phase 1.  V <= 64, so one 64-bit word.
 ORKAN_HD unsigned dm_get_local(unsigned x, const unsigned* vbit, unsigned k);
+inline unsigned long long dm_fixed_rows(const DmGeom& g) {
+    if (!g.fixmask) return 0ull;
+    unsigned long long m = 0;
+    for (unsigned x = 0; x < g.V(); ++x)
+        if ((g.fixmask >> dm_get_local(x, g.vbit, g.k)) & 1u) m |= 1ull << x;
+    return m;
+}
 
-// Is the element at virtual (vr, vc) unchanged by the gate (row and column fixed)?
-ORKAN_HD bool dm_fixed(const DmGeom& g, unsigned vr, unsigned vc) {
-    if (!g.fixmask) return false;
-    return ((g.fixmask >> dm_get_local(vr, g.vbit, g.k)) & (g.fixmask >> dm_get_local(vc, g.vbit, g.k)) & 1u) != 0;
+// Build the descriptors of item w (threads tid < 4^h, one position each).
+template <class Map>
+ORKAN_HD void dm_setup(const Map& map, const DmGeom& g, idx_t w, DmPos* pd, unsigned tid, unsigned nthr) {
+    const unsigned h = g.h, ls = g.ls, S = g.S(), P = g.P();
+    const unsigned npos = 1u << (2 * h);
+    if (tid >= npos) return;
+    idx_t u, v;
+    tri_unrank(w, &u, &v);
+    const bool diag_item = (u == v);
+    const idx_t rb = insert0_sorted(u, g.hb, h), cb = insert0_sorted(v, g.hb, h);
+    for (unsigned t = tid; t < npos; t += nthr) {
+        const unsigned a = t >> h, b = t & ((1u << h) - 1);
+        const idx_t R = (rb | spread_bits(a, g.hb, h)) << ls;
+        const idx_t C = (cb | spread_bits(b, g.hb, h)) << ls;
+        DmPos q;
+        q.mbase = 0;
+        q.gcol = 0;
+        q.has_c = 0;
+        q.mirror = 0;
+        q.pad_ = 0;
+        q.d0 = q.dl = q.dp = q.c0 = q.cl = q.cp = 0;
+        q.fconst = q.fvar = 0;
+        const int aS = (int)(a * S), bS = (int)(b * S);
+        if (R > C) {
+            q.cls = kSubDirect;
+            q.gbase = map.at(R, C);
+            q.has_c = diag_item ? 1 : 0;
+            if (Map::kRowContig) {       // packed: line = column j, p = row i
+                q.d0 = aS * (int)P + bS; q.dl = 1; q.dp = (int)P;
+                q.c0 = bS * (int)P + aS; q.cl = (int)P; q.cp = 1;
+                q.fconst = bS; q.fvar = aS;
+                q.gcol = map.d - C - 1;
+            } else {                     // tiled: line = row i, p = column j
+                q.d0 = aS * (int)P + bS; q.dl = (int)P; q.dp = 1;
+                q.c0 = bS * (int)P + aS; q.cl = 1; q.cp = (int)P;
+                q.fconst = aS; q.fvar = bS;
+                if (map.same_storage_block(R, C)) { q.mirror = 1; q.mbase = map.at(C, R); }
+            }
+        } else if (R == C) {
+            q.cls = kSubDiag;
+            q.gbase = map.at(R, R);
+            q.d0 = aS * (int)P + aS;
+            q.c0 = aS * (int)P + aS;
+            q.fconst = aS; q.fvar = aS;
+            if (Map::kRowContig) { q.dl = 1; q.dp = (int)P; q.cl = (int)P; q.cp = 1; q.gcol = map.d - R - 1; }
+            else                 { q.dl = (int)P; q.dp = 1; q.cl = 1; q.cp = (int)P; }
+        } else if (!diag_item) {
+            q.cls = kSubTransposed;
+            q.gbase = map.at(C, R);      // stored partner (C, R)
+            if (Map::kRowContig) {       // stored (C + p, R + line) is virtual (aS + line, bS + p), conjugated
+                q.c0 = aS * (int)P + bS; q.cl = (int)P; q.cp = 1;
+                q.fconst = aS; q.fvar = bS;
+                q.gcol = map.d - R - 1;
+            } else {                     // stored (C + line, R + p) is virtual (aS + p, bS + line), conjugated
+                q.c0 = aS * (int)P + bS; q.cl = 1; q.cp = (int)P;
+                q.fconst = bS; q.fvar = aS;
+                if (map.same_storage_block(C, R)) { q.mirror = 1; q.mbase = map.at(R, C); }
+            }
+        } else {
+            q.cls = kSubSkip;
+            q.gbase = 0;
+        }
+        pd[t] = q;
+    }
+}
+
+// Storage index of element (line, p) of a position's stored sub-tile.
+template <class Map>
+ORKAN_HD idx_t dm_addr(const Map& map, const DmPos& q, unsigned line, unsigned p) {
+    if (Map::kRowContig) return q.gbase + (idx_t)line * q.gcol - (idx_t)((line * (line - 1)) >> 1) + p;
+    return q.gbase + ((idx_t)line << map.log_tdim()) + p;
+}
+
+ORKAN_HD bool dm_skip(unsigned long long fm, const DmPos& q, unsigned line, unsigned p) {
+    return fm && ((fm >> (q.fconst + line)) & (fm >> (q.fvar + p)) & 1ull);
+}
+
+// Load rules: which of the element's slots the load fills (bit 0 direct, bit 1 conjugate).
+template <class Map>
+ORKAN_HD unsigned dm_load_slots(const DmPos& q, unsigned line, unsigned p) {
+    switch (q.cls) {
+        case kSubDirect: return 1u | (q.has_c ? 2u : 0u);
+        case kSubTransposed: return 2u;
+        case kSubDiag:
+            if (Map::kRowContig) return p >= line ? (1u | (p > line ? 2u : 0u)) : 0u;
+            return p <= line ? (1u | (p < line ? 2u : 0u)) : 0u;
+        default: return 0u;
+    }
 }
 
 // Stage one item into the shared block vb (pitch P).  Each thread first issues all of
-// its global loads (up to kDmMaxElems / kDmThreads = 16, so a block keeps its whole 64 KB
-// item in flight), then writes them to shared memory.
+// its global loads (up to kDmMaxElems / kDmThreads = 16, so a block keeps its whole item
+// in flight), then writes them to shared memory.
 constexpr unsigned kDmEpt = kDmMaxElems / kDmThreads;
-constexpr unsigned kNoSlot = 0xffffffffu;
 
 template <class Map, class Mem>
-ORKAN_HD void dm_load(const Mem& mem, const Map& map, const DmGeom& g, const DmItem& it,
-                      double2* vb, unsigned tid, unsigned nthr) {
-    const unsigned S = g.S(), P = g.P(), ls = g.ls, h = g.h;
-    const unsigned total = 1u << (2 * (ls + h));
+ORKAN_HD void dm_load(const Mem& mem, const Map& map, const DmGeom& g, const DmPos* pd, double2* vb,
+                      unsigned tid, unsigned nthr) {
+    const unsigned ls = g.ls, S = g.S();
+    const unsigned total = 1u << (2 * (ls + g.h));
+    const unsigned long long fm = g.fixrows;
     for (unsigned f0 = tid; f0 < total; f0 += nthr * kDmEpt) {
         double2 v[kDmEpt];
-        unsigned dst[kDmEpt], dstc[kDmEpt];   // direct / conjugated destination (kNoSlot = none)
+        unsigned slots[kDmEpt];   // direct slot (low 16 bits) and conjugate slot (high 16 bits); 0xffff = none
 #pragma unroll
         for (unsigned u = 0; u < kDmEpt; ++u) {
             const unsigned f = f0 + u * nthr;
-            dst[u] = kNoSlot;
-            dstc[u] = kNoSlot;
+            slots[u] = 0xffffffffu;
             if (f >= total) continue;
-            const unsigned pos = f >> (2 * ls), e = f & ((1u << (2 * ls)) - 1);
-            const unsigned a = pos >> h, b = pos & ((1u << h) - 1);
-            unsigned i, j;
-            dm_line_pos<Map>(e, ls, &i, &j);
-            const idx_t R = it.rseg[a], C = it.cseg[b];
-            switch (dm_sub_class(it, a, b)) {
-                case kSubDirect:
-                    if (dm_fixed(g, a * S + i, b * S + j)) break;
-                    v[u] = mem.ld(map.at(R + i, C + j));
-                    dst[u] = (a * S + i) * P + b * S + j;
-                    if (it.diag) dstc[u] = (b * S + j) * P + a * S + i;
-                    break;
-                case kSubDiag:
-                    if (i >= j && !dm_fixed(g, a * S + i, a * S + j)) {
-                        v[u] = mem.ld(map.at(R + i, R + j));
-                        dst[u] = (a * S + i) * P + a * S + j;
-                        if (i > j) dstc[u] = (a * S + j) * P + a * S + i;
-                    }
-                    break;
-                case kSubTransposed:
-                    // stored partner (C, R): its element (i, j) is virtual (R + j, C + i), conjugated
-                    if (dm_fixed(g, a * S + j, b * S + i)) break;
-                    v[u] = mem.ld(map.at(C + i, R + j));
-                    dstc[u] = (a * S + j) * P + b * S + i;
-                    break;
-                default:
-                    break;
-            }
+            const DmPos& q = pd[f >> (2 * ls)];
+            const unsigned e = f & ((1u << (2 * ls)) - 1), line = e >> ls, p = e & (S - 1);
+            const unsigned which = dm_load_slots<Map>(q, line, p);
+            if (!which || dm_skip(fm, q, line, p)) continue;
+            v[u] = mem.ld(dm_addr(map, q, line, p));
+            const unsigned sd = (which & 1u) ? (unsigned)(q.d0 + (int)line * q.dl + (int)p * q.dp) : 0xffffu;
+            const unsigned sc = (which & 2u) ? (unsigned)(q.c0 + (int)line * q.cl + (int)p * q.cp) : 0xffffu;
+            slots[u] = sd | (sc << 16);
         }
 #pragma unroll
         for (unsigned u = 0; u < kDmEpt; ++u) {
-            if (dst[u] != kNoSlot) vb[dst[u]] = v[u];
-            if (dstc[u] != kNoSlot) vb[dstc[u]] = cconj(v[u]);
+            const unsigned sd = slots[u] & 0xffffu, sc = slots[u] >> 16;
+            if (sd != 0xffffu) vb[sd] = v[u];
+            if (sc != 0xffffu) vb[sc] = cconj(v[u]);
         }
     }
 }
 
-// Write one item back (inverse of dm_load), regenerating tiled mirrors.
+// Write one item back, regenerating tiled mirrors and the upper half of diagonal tiles.
 template <class Map, class Mem>
-ORKAN_HD void dm_store(const Mem& mem, const Map& map, const DmGeom& g, const DmItem& it,
-                       const double2* vb, unsigned tid, unsigned nthr) {
-    const unsigned S = g.S(), P = g.P(), ls = g.ls, h = g.h;
-    const unsigned total = 1u << (2 * (ls + h));
+ORKAN_HD void dm_store(const Mem& mem, const Map& map, const DmGeom& g, const DmPos* pd, const double2* vb,
+                       unsigned tid, unsigned nthr) {
+    const unsigned ls = g.ls, S = g.S();
+    const unsigned total = 1u << (2 * (ls + g.h));
+    const unsigned long long fm = g.fixrows;
     for (unsigned f = tid; f < total; f += nthr) {
-        const unsigned pos = f >> (2 * ls), e = f & ((1u << (2 * ls)) - 1);
-        const unsigned a = pos >> h, b = pos & ((1u << h) - 1);
-        unsigned i, j;
-        dm_line_pos<Map>(e, ls, &i, &j);
-        const idx_t R = it.rseg[a], C = it.cseg[b];
-        switch (dm_sub_class(it, a, b)) {
-            case kSubDirect: {
-                if (dm_fixed(g, a * S + i, b * S + j)) break;
-                const double2 v = vb[(a * S + i) * P + b * S + j];
-                mem.st(map.at(R + i, C + j), v);
-                if (Map::kMirrors && map.same_storage_block(R, C)) mem.st(map.at(C + j, R + i), cconj(v));
-                break;
-            }
-            case kSubDiag: {
-                if (dm_fixed(g, a * S + i, a * S + j)) break;
-                if (i >= j) {
-                    mem.st(map.at(R + i, R + j), vb[(a * S + i) * P + a * S + j]);
-                } else if (Map::kMirrors) {
-                    mem.st(map.at(R + i, R + j), cconj(vb[(a * S + j) * P + a * S + i]));
-                }
-                break;
-            }
-            case kSubTransposed: {
-                if (dm_fixed(g, a * S + j, b * S + i)) break;
-                const double2 v = vb[(a * S + j) * P + b * S + i];
-                mem.st(map.at(C + i, R + j), cconj(v));
-                if (Map::kMirrors && map.same_storage_block(C, R)) mem.st(map.at(R + j, C + i), v);
-                break;
-            }
-            default:
-                break;
+        const DmPos& q = pd[f >> (2 * ls)];
+        if (q.cls == kSubSkip) continue;
+        const unsigned e = f & ((1u << (2 * ls)) - 1), line = e >> ls, p = e & (S - 1);
+        if (dm_skip(fm, q, line, p)) continue;
+        double2 val;
+        if (q.cls == kSubDirect) {
+            val = vb[q.d0 + (int)line * q.dl + (int)p * q.dp];
+        } else if (q.cls == kSubTransposed) {
+            val = cconj(vb[q.c0 + (int)line * q.cl + (int)p * q.cp]);
+        } else if (Map::kRowContig) {                   // packed diagonal sub-tile: lower half only
+            if (p < line) continue;
+            val = vb[q.d0 + (int)line * q.dl + (int)p * q.dp];
+        } else {                                        // tiled diagonal sub-tile: both halves
+            val = p <= line ? vb[q.d0 + (int)line * q.dl + (int)p * q.dp]
+                            : cconj(vb[q.c0 + (int)line * q.cl + (int)p * q.cp]);
         }
+        mem.st(dm_addr(map, q, line, p), val);
+        if (Map::kMirrors && q.mirror)
+            mem.st(q.mbase + ((idx_t)p << map.log_tdim()) + line, cconj(val));
     }
 }
 
@@ -380,25 +431,28 @@ inline unsigned monomial_fixmask(const OpMonomial& op, unsigned m) {
 
 // Kernel body for one work item, split into phases separated by block barriers.
 template <class Map, class Mem, class Op>
-ORKAN_HD void dm_engine_item_phase(int phase, const Mem& mem, const Map& map, const DmGeom& g,
-                                   const Op& op, const DmItem& it, double2* vb, unsigned tid, unsigned nthr) {
-    if (phase == 0) dm_load(mem, map, g, it, vb, tid, nthr);
-    else if (phase == 1) op(g, vb, tid, nthr);
-    else dm_store(mem, map, g, it, vb, tid, nthr);
+ORKAN_HD void dm_engine_item_phase(int phase, const Mem& mem, const Map& map, const DmGeom& g, const Op& op,
+                                   idx_t w, DmPos* pd, double2* vb, unsigned tid, unsigned nthr) {
+    if (phase == 0) dm_setup(map, g, w, pd, tid, nthr);
+    else if (phase == 1) dm_load(mem, map, g, pd, vb, tid, nthr);
+    else if (phase == 2) op(g, vb, tid, nthr);
+    else dm_store(mem, map, g, pd, vb, tid, nthr);
 }
 
 #ifdef __CUDACC__
 template <class Map, class Op>
 __global__ void __launch_bounds__(kDmThreads) k_dm_engine(DevMem mem, Map map, DmGeom g, Op op) {
-    extern __shared__ double2 vb[];
-    DmItem it;
+    extern __shared__ double2 smem[];
+    DmPos* pd = reinterpret_cast<DmPos*>(smem);
+    double2* vb = smem + kDmPosBytes / sizeof(double2);
     for (idx_t w = blockIdx.x; w < g.items; w += gridDim.x) {
-        dm_item(g, w, it);
-        dm_load(mem, map, g, it, vb, threadIdx.x, blockDim.x);
+        dm_setup(map, g, w, pd, threadIdx.x, blockDim.x);
+        __syncthreads();
+        dm_load(mem, map, g, pd, vb, threadIdx.x, blockDim.x);
         __syncthreads();
         op(g, vb, threadIdx.x, blockDim.x);
         __syncthreads();
-        dm_store(mem, map, g, it, vb, threadIdx.x, blockDim.x);
+        dm_store(mem, map, g, pd, vb, threadIdx.x, blockDim.x);
         __syncthreads();
     }
 }

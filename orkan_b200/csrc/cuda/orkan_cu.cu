@@ -53,7 +53,7 @@ inline double2 ld_c(const double* p, unsigned i) { return c2(p[2 * i], p[2 * i +
 template <class Op>
 int launch_engine_map(int layout, unsigned log_tile, void* rho, unsigned n, const DmGeom& g, const Op& op,
                       cudaStream_t st) {
-    const size_t smem = (size_t)g.V() * g.P() * sizeof(double2);
+    const size_t smem = dm_smem_bytes(g);
     const unsigned grid = grid_for(1, g.items, (unsigned)sm_count() * 32u);
     DevMem mem{static_cast<double2*>(rho)};
     if (layout == 1) {
@@ -208,6 +208,7 @@ int orkan_cu_dm_monomial(int layout, unsigned log_tile, void* rho, unsigned n, u
     DmGeom g;
     if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g)) return (int)cudaErrorInvalidValue;
     g.fixmask = monomial_fixmask(op, m);
+    g.fixrows = dm_fixed_rows(g);
     return launch_engine_map(layout, log_tile, rho, n, g, op, as_stream(stream));
 }
 

@@ -74,13 +74,12 @@ template <class Map, class Op>
 void run_engine(const EmuMem& mem, const Map& map, const DmGeom& g, const Op& op) {
     const unsigned grid = grid_for(1, g.items, kSms * 32u);
     std::vector<double2> vb((size_t)g.V() * g.P());
+    std::vector<DmPos> pd(kDmMaxPos);
     for (unsigned b = 0; b < grid; ++b) {
         for (idx_t w = b; w < g.items; w += grid) {
-            DmItem it;
-            dm_item(g, w, it);
-            for (int phase = 0; phase < 3; ++phase)
+            for (int phase = 0; phase < 4; ++phase)
                 for (unsigned t = 0; t < kDmThreads; ++t)
-                    dm_engine_item_phase(phase, mem, map, g, op, it, vb.data(), t, kDmThreads);
+                    dm_engine_item_phase(phase, mem, map, g, op, w, pd.data(), vb.data(), t, kDmThreads);
         }
     }
 }
@@ -100,12 +99,15 @@ template <class Factor>
 void run_phase(int layout, unsigned log_tile, const EmuMem& mem, unsigned n, const Factor& fac) {
     const PhaseGeom g = phase_geometry(n, layout == 2 ? log_tile : 5u);
     const unsigned grid = grid_for(1, g.items, kSms * 32u);
+    PhaseShared sh;
     for (unsigned b = 0; b < grid; ++b)
-        for (idx_t w = b; w < g.items; w += grid)
+        for (idx_t w = b; w < g.items; w += grid) {
+            for (unsigned t = 0; t < kPhaseThreads; ++t) dm_phase_setup(g, fac, w, &sh, t, kPhaseThreads);
             for (unsigned t = 0; t < kPhaseThreads; ++t) {
-                if (layout == 1) dm_phase_item(mem, PackedMap{idx_t(1) << n}, g, fac, w, t, kPhaseThreads);
-                else dm_phase_item(mem, TiledMap{idx_t(1) << n, log_tile}, g, fac, w, t, kPhaseThreads);
+                if (layout == 1) dm_phase_item(mem, PackedMap{idx_t(1) << n}, g, fac, &sh, w, t, kPhaseThreads);
+                else dm_phase_item(mem, TiledMap{idx_t(1) << n, log_tile}, g, fac, &sh, w, t, kPhaseThreads);
             }
+        }
 }
 
 }  // namespace
@@ -139,6 +141,7 @@ int emu_dm_monomial(int layout, unsigned log_tile, double* rho, uint64_t len, un
     DmGeom g;
     if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g)) return -1;
     g.fixmask = monomial_fixmask(op, 1u << k);
+    g.fixrows = dm_fixed_rows(g);
     return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
 }
 

@@ -169,3 +169,25 @@ def test_fill_emulated(kind, lt, n):
     assert res.oob == 0
     exp = R.to_storage(kind, np.full(d if kind == "pure" else (d, d), 0.25, dtype=complex), lt)
     assert np.array_equal(res.out, exp)
+
+
+@pytest.mark.parametrize("lt", [6, 7])
+@pytest.mark.parametrize("n", [3, 6, 8])
+def test_tiles_larger_than_phase_subtile_emulated(lt, n):
+    """Tile sides of 64 and 128 (LOG_TILE_DIM 6, 7): sub-tiles smaller than a tile, so
+    off-diagonal sub-tiles of a diagonal tile need their mirror rewritten."""
+    rng = np.random.default_rng(lt * 10 + n)
+    rho = rand_rho(n, 700 + n)
+    st = R.to_storage("tiled", rho, lt)
+    for g in ("z", "t", "rz", "cz", "h", "cx", "swap", "ccx", "ry"):
+        k = W.gate_arity(g)
+        if k > n:
+            continue
+        qs = tuple(int(q) for q in rng.choice(n, k, replace=False))
+        th = 0.4 if g in W.GATES_ROT else None
+        res = kemu.dm_gate("tiled", lt, st, n, g, qs, th)
+        exp = R.to_storage("tiled", R.apply_mixed(rho, g, qs, th), lt)
+        assert res.oob == 0 and np.abs(res.out - exp).max() <= TOL, (g, qs)
+    diag = rng.uniform(-2, 2, 1 << n)
+    res = kemu.dm_exp_diag("tiled", lt, st, n, diag, 0.3)
+    assert np.abs(res.out - R.to_storage("tiled", R.exp_diag("tiled", rho, diag, 0.3), lt)).max() <= TOL
