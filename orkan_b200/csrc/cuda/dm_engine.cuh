@@ -227,40 +227,41 @@ ORKAN_HD unsigned dm_load_slots(const DmPos& q, unsigned line, unsigned p) {
     }
 }
 
-// Stage one item into the shared block vb (pitch P).  Each thread first issues all of
-// its global loads (up to kDmMaxElems / kDmThreads = 16, so a block keeps its whole item
-// in flight), then writes them to shared memory.
-constexpr unsigned kDmEpt = kDmMaxElems / kDmThreads;
-
+// Stage one item into the shared block vb (pitch P) with asynchronous 16-byte global->shared
+// copies (cp.async): no register staging, so a block keeps a whole item in flight while it
+// computes and stores the previous one.  An element that must also appear conjugated
+// (upper half of a diagonal sub-tile, the transposed copy of a sub-tile of a diagonal
+// item, every element of a transposed sub-tile) is copied raw into its conjugate slot and
+// fixed up by the same thread after its copies have landed (dm_fixup).
 template <class Map, class Mem>
-ORKAN_HD void dm_load(const Mem& mem, const Map& map, const DmGeom& g, const DmPos* pd, double2* vb,
-                      unsigned tid, unsigned nthr) {
+ORKAN_HD void dm_issue(const Mem& mem, const Map& map, const DmGeom& g, const DmPos* pd, double2* vb,
+                       unsigned tid, unsigned nthr) {
     const unsigned ls = g.ls, S = g.S();
     const unsigned total = 1u << (2 * (ls + g.h));
     const unsigned long long fm = g.fixrows;
-    for (unsigned f0 = tid; f0 < total; f0 += nthr * kDmEpt) {
-        double2 v[kDmEpt];
-        unsigned slots[kDmEpt];   // direct slot (low 16 bits) and conjugate slot (high 16 bits); 0xffff = none
-#pragma unroll
-        for (unsigned u = 0; u < kDmEpt; ++u) {
-            const unsigned f = f0 + u * nthr;
-            slots[u] = 0xffffffffu;
-            if (f >= total) continue;
-            const DmPos& q = pd[f >> (2 * ls)];
-            const unsigned e = f & ((1u << (2 * ls)) - 1), line = e >> ls, p = e & (S - 1);
-            const unsigned which = dm_load_slots<Map>(q, line, p);
-            if (!which || dm_skip(fm, q, line, p)) continue;
-            v[u] = mem.ld(dm_addr(map, q, line, p));
-            const unsigned sd = (which & 1u) ? (unsigned)(q.d0 + (int)line * q.dl + (int)p * q.dp) : 0xffffu;
-            const unsigned sc = (which & 2u) ? (unsigned)(q.c0 + (int)line * q.cl + (int)p * q.cp) : 0xffffu;
-            slots[u] = sd | (sc << 16);
-        }
-#pragma unroll
-        for (unsigned u = 0; u < kDmEpt; ++u) {
-            const unsigned sd = slots[u] & 0xffffu, sc = slots[u] >> 16;
-            if (sd != 0xffffu) vb[sd] = v[u];
-            if (sc != 0xffffu) vb[sc] = cconj(v[u]);
-        }
+    for (unsigned f = tid; f < total; f += nthr) {
+        const DmPos& q = pd[f >> (2 * ls)];
+        const unsigned e = f & ((1u << (2 * ls)) - 1), line = e >> ls, p = e & (S - 1);
+        const unsigned which = dm_load_slots<Map>(q, line, p);
+        if (!which || dm_skip(fm, q, line, p)) continue;
+        const idx_t a = dm_addr(map, q, line, p);
+        if (which & 1u) mem.cp(vb + (q.d0 + (int)line * q.dl + (int)p * q.dp), a);
+        if (which & 2u) mem.cp(vb + (q.c0 + (int)line * q.cl + (int)p * q.cp), a);
+    }
+}
+
+// Conjugate the slots this thread filled through its conjugate copies (after they landed).
+template <class Map>
+ORKAN_HD void dm_fixup(const DmGeom& g, const DmPos* pd, double2* vb, unsigned tid, unsigned nthr) {
+    const unsigned ls = g.ls, S = g.S();
+    const unsigned total = 1u << (2 * (ls + g.h));
+    const unsigned long long fm = g.fixrows;
+    for (unsigned f = tid; f < total; f += nthr) {
+        const DmPos& q = pd[f >> (2 * ls)];
+        const unsigned e = f & ((1u << (2 * ls)) - 1), line = e >> ls, p = e & (S - 1);
+        if (!(dm_load_slots<Map>(q, line, p) & 2u) || dm_skip(fm, q, line, p)) continue;
+        double2& x = vb[q.c0 + (int)line * q.cl + (int)p * q.cp];
+        x.y = -x.y;
     }
 }
 
@@ -429,32 +430,67 @@ inline unsigned monomial_fixmask(const OpMonomial& op, unsigned m) {
     return mask;
 }
 
-// Kernel body for one work item, split into phases separated by block barriers.
+// One work item, phase by phase (the CPU emulator runs each phase for all threads
+// before the next; the kernel below overlaps items with a two-stage pipeline).
 template <class Map, class Mem, class Op>
 ORKAN_HD void dm_engine_item_phase(int phase, const Mem& mem, const Map& map, const DmGeom& g, const Op& op,
                                    idx_t w, DmPos* pd, double2* vb, unsigned tid, unsigned nthr) {
     if (phase == 0) dm_setup(map, g, w, pd, tid, nthr);
-    else if (phase == 1) dm_load(mem, map, g, pd, vb, tid, nthr);
-    else if (phase == 2) op(g, vb, tid, nthr);
+    else if (phase == 1) dm_issue(mem, map, g, pd, vb, tid, nthr);
+    else if (phase == 2) dm_fixup<Map>(g, pd, vb, tid, nthr);
+    else if (phase == 3) op(g, vb, tid, nthr);
     else dm_store(mem, map, g, pd, vb, tid, nthr);
 }
 
+constexpr unsigned kDmBlock = 512;          // threads of the pipelined engine block
+
+// Shared memory of one pipelined block: two descriptor sets and two staged blocks.
+ORKAN_HD size_t dm_pipe_smem_bytes(const DmGeom& g) { return 2 * dm_smem_bytes(g); }
+
 #ifdef __CUDACC__
-template <class Map, class Op>
-__global__ void __launch_bounds__(kDmThreads) k_dm_engine(DevMem mem, Map map, DmGeom g, Op op) {
-    extern __shared__ double2 smem[];
-    DmPos* pd = reinterpret_cast<DmPos*>(smem);
-    double2* vb = smem + kDmPosBytes / sizeof(double2);
-    for (idx_t w = blockIdx.x; w < g.items; w += gridDim.x) {
-        dm_setup(map, g, w, pd, threadIdx.x, blockDim.x);
-        __syncthreads();
-        dm_load(mem, map, g, pd, vb, threadIdx.x, blockDim.x);
-        __syncthreads();
-        op(g, vb, threadIdx.x, blockDim.x);
-        __syncthreads();
-        dm_store(mem, map, g, pd, vb, threadIdx.x, blockDim.x);
-        __syncthreads();
+struct DevMemAsync : DevMem {
+    __device__ __forceinline__ void cp(double2* sdst, idx_t i) const {
+        const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(p + i) : "memory");
     }
+};
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Persistent, double-buffered engine: block b handles items b, b + G, b + 2G, ...; the
+// copies of the next item are in flight while the current one is computed and stored.
+template <class Map, class Op>
+__global__ void __launch_bounds__(kDmBlock) k_dm_engine(DevMemAsync mem, Map map, DmGeom g, Op op) {
+    extern __shared__ double2 smem[];
+    const size_t half = dm_smem_bytes(g) / sizeof(double2);
+    DmPos* pd[2] = {reinterpret_cast<DmPos*>(smem), reinterpret_cast<DmPos*>(smem + half)};
+    double2* vb[2] = {smem + kDmPosBytes / sizeof(double2), smem + half + kDmPosBytes / sizeof(double2)};
+    const unsigned tid = threadIdx.x, nthr = blockDim.x;
+    idx_t w = blockIdx.x;
+    if (w >= g.items) return;
+    dm_setup(map, g, w, pd[0], tid, nthr);
+    __syncthreads();
+    dm_issue(mem, map, g, pd[0], vb[0], tid, nthr);
+    cp_commit();
+    for (unsigned it = 0;; ++it) {
+        const unsigned cur = it & 1u, nxt = cur ^ 1u;
+        const idx_t wn = w + gridDim.x;
+        if (wn < g.items) dm_setup(map, g, wn, pd[nxt], tid, nthr);
+        __syncthreads();                                  // pd[nxt] ready; vb[nxt] free
+        if (wn < g.items) dm_issue(mem, map, g, pd[nxt], vb[nxt], tid, nthr);
+        cp_commit();
+        cp_wait<1>();                                     // this thread's copies of item w landed
+        dm_fixup<Map>(g, pd[cur], vb[cur], tid, nthr);
+        __syncthreads();
+        op(g, vb[cur], tid, nthr);
+        __syncthreads();
+        dm_store(mem, map, g, pd[cur], vb[cur], tid, nthr);
+        if (wn >= g.items) break;
+        w = wn;
+        __syncthreads();                                  // vb[cur], pd[cur] free for item w + 2G
+    }
+    cp_wait<0>();
 }
 #endif
 

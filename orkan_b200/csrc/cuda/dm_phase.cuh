@@ -16,7 +16,7 @@
 
 namespace orkan {
 
-constexpr unsigned kPhaseThreads = 256;
+constexpr unsigned kPhaseThreads = 128;
 
 struct PhaseGeom {
     idx_t d;
@@ -36,21 +36,43 @@ inline PhaseGeom phase_geometry(unsigned n, unsigned ls_max) {
     return g;
 }
 
-// Phase of a k-qubit diagonal gate: phi(x) = phase[local(x)], local(x) = sum_j bit(x, q[j]) << (k-1-j).
-// The element factor is phi(r) conj(phi(c)); rows and columns with the same local index
-// get factor |phi|^2 = 1 and are skipped.
+// Factor forms.  factor(r, c, &f) returns false when the element is unchanged.
+//
+// 1-qubit diagonal gate diag(1, ph1) on qubit q: f = ph1 when bit q of r is set and of c
+// clear, conj(ph1) in the opposite case, unchanged otherwise.
+struct GateFactor1 {
+    unsigned q;
+    double2 ph1;
+    ORKAN_HD bool factor(idx_t r, idx_t c, double2* f) const {
+        const unsigned br = (unsigned)(r >> q) & 1u, bc = (unsigned)(c >> q) & 1u;
+        if (br == bc) return false;
+        *f = br ? ph1 : cconj(ph1);
+        return true;
+    }
+};
+
+// k-qubit diagonal gate (k <= 3): phi(x) = phase[local(x)], local(x) = sum_j bit(x, q[j]) << (k-1-j);
+// f = phi(r) conj(phi(c)); equal local indices give |phi|^2 = 1 and are skipped.
 struct GateFactor {
     unsigned k;
     unsigned q[3];
     double2 phase[8];
-    static constexpr bool kKeyed = true;
-    ORKAN_HD unsigned key(idx_t x) const {
+    ORKAN_HD unsigned local(idx_t x) const {
         unsigned l = 0;
         for (unsigned j = 0; j < k; ++j) l = (l << 1) | (unsigned)((x >> q[j]) & 1u);
         return l;
     }
-    ORKAN_HD double2 value(idx_t x) const { return phase[key(x)]; }
-    ORKAN_HD double2 combine(double2 rv, double2 cv) const { return cmulc(rv, cv); }
+    ORKAN_HD bool factor(idx_t r, idx_t c, double2* f) const {
+        const unsigned lr = local(r), lc = local(c);
+        if (lr == lc) return false;
+        double2 pr = phase[0], pc = phase[0];
+        for (unsigned l = 1; l < 8; ++l) {      // select without dynamic indexing
+            if (l == lr) pr = phase[l];
+            if (l == lc) pc = phase[l];
+        }
+        *f = cmulc(pr, pc);
+        return !(f->x == 1.0 && f->y == 0.0);
+    }
 };
 
 // exp_diag: tab[x] = (cos(diag[x] t), sin(diag[x] t)); the factor e^{-i(d_r - d_c)t} is
@@ -58,10 +80,12 @@ struct GateFactor {
 template <class MemR2>
 struct TableFactor {
     MemR2 tab;
-    static constexpr bool kKeyed = false;
-    ORKAN_HD unsigned key(idx_t) const { return 0; }
-    ORKAN_HD double2 value(idx_t x) const { return tab.ld(x); }
-    ORKAN_HD double2 combine(double2 rv, double2 cv) const { return cmulc(cv, rv); }
+    ORKAN_HD bool factor(idx_t r, idx_t c, double2* f) const {
+        const double2 pr = tab.ld(r), pc = tab.ld(c);
+        f->x = pr.x * pc.x + pr.y * pc.y;
+        f->y = -pr.y * pc.x + pr.x * pc.y;
+        return true;
+    }
 };
 
 // Apply rho' = f * rho  (complex product written out as the reference does:
@@ -70,39 +94,23 @@ ORKAN_HD double2 phase_apply(double2 f, double2 v) {
     return c2(f.x * v.x - f.y * v.y, f.x * v.y + f.y * v.x);
 }
 
-constexpr unsigned kPhaseMaxS = 32;   // sub-tile side of the phase pass
-constexpr unsigned kPhaseEpt = 4;     // elements per thread per trip: loads issued together
+constexpr unsigned kPhaseEpt = 8;     // elements per thread per trip: loads issued together
 
-// Per-item staging in shared memory: factor values and skip keys of the S rows and S columns.
-struct PhaseShared {
-    double2 rv[kPhaseMaxS], cv[kPhaseMaxS];
-    unsigned char rk[kPhaseMaxS], ck[kPhaseMaxS];
-};
-
-template <class Factor>
-ORKAN_HD void dm_phase_setup(const PhaseGeom& g, const Factor& fac, idx_t w, PhaseShared* sh, unsigned tid,
-                             unsigned nthr) {
-    idx_t u, v;
-    tri_unrank(w, &u, &v);
-    const unsigned S = 1u << g.ls;
-    for (unsigned t = tid; t < 2 * S; t += nthr) {
-        if (t < S) {
-            const idx_t r = (u << g.ls) + t;
-            sh->rv[t] = fac.value(r);
-            sh->rk[t] = (unsigned char)fac.key(r);
-        } else {
-            const idx_t c = (v << g.ls) + (t - S);
-            sh->cv[t - S] = fac.value(c);
-            sh->ck[t - S] = (unsigned char)fac.key(c);
-        }
-    }
+// Row u, column v of the lower-triangular item index w = u(u+1)/2 + v (single-precision
+// estimate, corrected exactly in integers).
+ORKAN_HD void tri_unrank_fast(idx_t w, idx_t* u, idx_t* v) {
+    idx_t uu = (idx_t)((sqrtf(8.0f * (float)w + 1.0f) - 1.0f) * 0.5f);
+    while (uu > 0 && uu * (uu + 1) / 2 > w) --uu;
+    while ((uu + 1) * (uu + 2) / 2 <= w) ++uu;
+    *u = uu;
+    *v = w - uu * (uu + 1) / 2;
 }
 
 template <class Map, class Mem, class Factor>
 ORKAN_HD void dm_phase_item(const Mem& mem, const Map& map, const PhaseGeom& g, const Factor& fac,
-                            const PhaseShared* sh, idx_t w, unsigned tid, unsigned nthr) {
+                            idx_t w, unsigned tid, unsigned nthr) {
     idx_t u, v;
-    tri_unrank(w, &u, &v);
+    tri_unrank_fast(w, &u, &v);
     const unsigned ls = g.ls, S = 1u << ls;
     const idx_t R = u << ls, C = v << ls;
     const unsigned total = S * S;
@@ -110,12 +118,12 @@ ORKAN_HD void dm_phase_item(const Mem& mem, const Map& map, const PhaseGeom& g, 
     const idx_t base = map.at(R, C);
     const idx_t gcol = Map::kRowContig ? map.d - C - 1 : 0;
     const unsigned lt = map.log_tdim();
-    // tiled: the item lies in a diagonal tile, so its mirror image is stored too
+    // tiled: an item inside a diagonal tile has its mirror image stored too
     const bool mir = Map::kMirrors && (diag || map.same_storage_block(R, C));
     const idx_t mbase = diag ? base : (mir ? map.at(C, R) : 0);
     for (unsigned e0 = tid; e0 < total; e0 += nthr * kPhaseEpt) {
         idx_t addr[kPhaseEpt];
-        double2 val[kPhaseEpt];
+        double2 val[kPhaseEpt], f[kPhaseEpt];
         unsigned ij[kPhaseEpt];
         bool act[kPhaseEpt];
 #pragma unroll
@@ -127,9 +135,9 @@ ORKAN_HD void dm_phase_item(const Mem& mem, const Map& map, const PhaseGeom& g, 
             unsigned i, j;
             if (Map::kRowContig) { i = p; j = line; } else { i = line; j = p; }
             if (diag && i <= j) continue;
-            if (Factor::kKeyed && sh->rk[i] == sh->ck[j]) continue;
+            if (!fac.factor(R + i, C + j, &f[k])) continue;
             act[k] = true;
-            ij[k] = (i << 8) | j;
+            ij[k] = (i << 16) | j;
             addr[k] = Map::kRowContig ? base + (idx_t)line * gcol - (idx_t)((line * (line - 1)) >> 1) + p
                                       : base + ((idx_t)line << lt) + p;
             val[k] = mem.ld(addr[k]);
@@ -137,10 +145,9 @@ ORKAN_HD void dm_phase_item(const Mem& mem, const Map& map, const PhaseGeom& g, 
 #pragma unroll
         for (unsigned k = 0; k < kPhaseEpt; ++k) {
             if (!act[k]) continue;
-            const unsigned i = ij[k] >> 8, j = ij[k] & 0xffu;
-            const double2 nv = phase_apply(fac.combine(sh->rv[i], sh->cv[j]), val[k]);
+            const double2 nv = phase_apply(f[k], val[k]);
             mem.st(addr[k], nv);
-            if (Map::kMirrors && mir) mem.st(mbase + ((idx_t)j << lt) + i, cconj(nv));
+            if (Map::kMirrors && mir) mem.st(mbase + ((idx_t)(ij[k] & 0xffffu) << lt) + (ij[k] >> 16), cconj(nv));
         }
     }
 }
@@ -148,13 +155,8 @@ ORKAN_HD void dm_phase_item(const Mem& mem, const Map& map, const PhaseGeom& g, 
 #ifdef __CUDACC__
 template <class Map, class Factor>
 __global__ void __launch_bounds__(kPhaseThreads) k_dm_phase(DevMem mem, Map map, PhaseGeom g, Factor fac) {
-    __shared__ PhaseShared sh;
-    for (idx_t w = blockIdx.x; w < g.items; w += gridDim.x) {
-        dm_phase_setup(g, fac, w, &sh, threadIdx.x, blockDim.x);
-        __syncthreads();
-        dm_phase_item(mem, map, g, fac, &sh, w, threadIdx.x, blockDim.x);
-        __syncthreads();
-    }
+    for (idx_t w = blockIdx.x; w < g.items; w += gridDim.x)
+        dm_phase_item(mem, map, g, fac, w, threadIdx.x, blockDim.x);
 }
 #endif
 

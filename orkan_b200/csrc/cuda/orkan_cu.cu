@@ -50,24 +50,33 @@ struct Complex8 { double2 v[8]; };
 inline double2 ld_c(const double* p, unsigned i) { return c2(p[2 * i], p[2 * i + 1]); }
 
 // ---- density-matrix engine dispatch -------------------------------------------------
+template <class Kern>
+unsigned engine_grid(Kern kern, size_t smem, idx_t items) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * (int)(kDmPosBytes + 64 * 65 * 16));
+        attr = true;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kDmBlock, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return grid_for(1, items, (unsigned)(sm_count() * per_sm));
+}
+
 template <class Op>
 int launch_engine_map(int layout, unsigned log_tile, void* rho, unsigned n, const DmGeom& g, const Op& op,
                       cudaStream_t st) {
-    const size_t smem = dm_smem_bytes(g);
-    const unsigned grid = grid_for(1, g.items, (unsigned)sm_count() * 32u);
-    DevMem mem{static_cast<double2*>(rho)};
+    const size_t smem = dm_pipe_smem_bytes(g);
+    DevMemAsync mem;
+    mem.p = static_cast<double2*>(rho);
     if (layout == 1) {
-        PackedMap map{idx_t(1) << n};
         auto kern = k_dm_engine<PackedMap, Op>;
-        static bool attr = false;
-        if (!attr) { cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024); attr = true; }
-        kern<<<grid, kDmThreads, smem, st>>>(mem, map, g, op);
+        const unsigned grid = engine_grid(kern, smem, g.items);
+        kern<<<grid, kDmBlock, smem, st>>>(mem, PackedMap{idx_t(1) << n}, g, op);
     } else {
-        TiledMap map{idx_t(1) << n, log_tile};
         auto kern = k_dm_engine<TiledMap, Op>;
-        static bool attr = false;
-        if (!attr) { cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024); attr = true; }
-        kern<<<grid, kDmThreads, smem, st>>>(mem, map, g, op);
+        const unsigned grid = engine_grid(kern, smem, g.items);
+        kern<<<grid, kDmBlock, smem, st>>>(mem, TiledMap{idx_t(1) << n, log_tile}, g, op);
     }
     return finish_launch();
 }
@@ -216,13 +225,17 @@ int orkan_cu_dm_phase(int layout, unsigned log_tile, void* rho, unsigned n, unsi
                       const double* phase, void* stream) {
     if (!rho || !qubits || !phase || !layout_ok(layout, log_tile) || k < 1 || k > 3 || n > 40)
         return (int)cudaErrorInvalidValue;
+    for (unsigned j = 0; j < k; ++j)
+        if (qubits[j] >= n) return (int)cudaErrorInvalidValue;
+    if (k == 1 && phase[0] == 1.0 && phase[1] == 0.0) {
+        GateFactor1 f1;
+        f1.q = qubits[0];
+        f1.ph1 = ld_c(phase, 1);
+        return launch_phase(layout, log_tile, rho, n, f1, as_stream(stream));
+    }
     GateFactor fac;
     fac.k = k;
-    for (unsigned j = 0; j < 3; ++j) fac.q[j] = 0;
-    for (unsigned j = 0; j < k; ++j) {
-        if (qubits[j] >= n) return (int)cudaErrorInvalidValue;
-        fac.q[j] = qubits[j];
-    }
+    for (unsigned j = 0; j < 3; ++j) fac.q[j] = j < k ? qubits[j] : 0;
     for (unsigned y = 0; y < 8; ++y) fac.phase[y] = y < (1u << k) ? ld_c(phase, y) : c2(1.0, 0.0);
     return launch_phase(layout, log_tile, rho, n, fac, as_stream(stream));
 }

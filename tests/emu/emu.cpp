@@ -37,6 +37,15 @@ struct EmuMem {
         ++writes[i];
         p[i] = v;
     }
+    // asynchronous copy of the GPU path: lands immediately here; counted as one read per
+    // element even when an element is copied to two shared-memory slots
+    void cp(double2* dst, idx_t i) const {
+        if (i >= len) { ++*oob; return; }
+        if (i != last_cp) ++reads[i];
+        last_cp = i;
+        *dst = p[i];
+    }
+    mutable idx_t last_cp = ~idx_t(0);
 };
 
 struct EmuMemR {
@@ -77,9 +86,9 @@ void run_engine(const EmuMem& mem, const Map& map, const DmGeom& g, const Op& op
     std::vector<DmPos> pd(kDmMaxPos);
     for (unsigned b = 0; b < grid; ++b) {
         for (idx_t w = b; w < g.items; w += grid) {
-            for (int phase = 0; phase < 4; ++phase)
-                for (unsigned t = 0; t < kDmThreads; ++t)
-                    dm_engine_item_phase(phase, mem, map, g, op, w, pd.data(), vb.data(), t, kDmThreads);
+            for (int phase = 0; phase < 5; ++phase)
+                for (unsigned t = 0; t < kDmBlock; ++t)
+                    dm_engine_item_phase(phase, mem, map, g, op, w, pd.data(), vb.data(), t, kDmBlock);
         }
     }
 }
@@ -99,15 +108,12 @@ template <class Factor>
 void run_phase(int layout, unsigned log_tile, const EmuMem& mem, unsigned n, const Factor& fac) {
     const PhaseGeom g = phase_geometry(n, layout == 2 ? log_tile : 5u);
     const unsigned grid = grid_for(1, g.items, kSms * 32u);
-    PhaseShared sh;
     for (unsigned b = 0; b < grid; ++b)
-        for (idx_t w = b; w < g.items; w += grid) {
-            for (unsigned t = 0; t < kPhaseThreads; ++t) dm_phase_setup(g, fac, w, &sh, t, kPhaseThreads);
+        for (idx_t w = b; w < g.items; w += grid)
             for (unsigned t = 0; t < kPhaseThreads; ++t) {
-                if (layout == 1) dm_phase_item(mem, PackedMap{idx_t(1) << n}, g, fac, &sh, w, t, kPhaseThreads);
-                else dm_phase_item(mem, TiledMap{idx_t(1) << n, log_tile}, g, fac, &sh, w, t, kPhaseThreads);
+                if (layout == 1) dm_phase_item(mem, PackedMap{idx_t(1) << n}, g, fac, w, t, kPhaseThreads);
+                else dm_phase_item(mem, TiledMap{idx_t(1) << n, log_tile}, g, fac, w, t, kPhaseThreads);
             }
-        }
 }
 
 }  // namespace
@@ -157,11 +163,18 @@ int emu_dm_superop1(int layout, unsigned log_tile, double* rho, uint64_t len, un
 
 int emu_dm_phase(int layout, unsigned log_tile, double* rho, uint64_t len, unsigned n, unsigned k,
                  const unsigned* qubits, const double* phase, uint32_t* reads, uint32_t* writes, uint64_t* oob) {
+    EmuMem mem{reinterpret_cast<double2*>(rho), len, reads, writes, oob};
+    if (k == 1 && phase[0] == 1.0 && phase[1] == 0.0) {
+        GateFactor1 f1;
+        f1.q = qubits[0];
+        f1.ph1 = ldc(phase, 1);
+        run_phase(layout, log_tile, mem, n, f1);
+        return 0;
+    }
     GateFactor fac;
     fac.k = k;
     for (unsigned j = 0; j < 3; ++j) fac.q[j] = j < k ? qubits[j] : 0;
     for (unsigned y = 0; y < 8; ++y) fac.phase[y] = y < (1u << k) ? ldc(phase, y) : c2(1.0, 0.0);
-    EmuMem mem{reinterpret_cast<double2*>(rho), len, reads, writes, oob};
     run_phase(layout, log_tile, mem, n, fac);
     return 0;
 }
