@@ -95,6 +95,21 @@ int orkan_cu_mean(int layout, unsigned log_tile, const void *data, unsigned n, c
 int orkan_cu_matel_diag(const void *bra, const void *ket, unsigned n, const double *obs,
                         double *result, void *stream);
 
+/* exp_diag on a MIXED_PACKED (layout 1) or MIXED_TILED (layout 2) density matrix that
+ * allocates nothing.  No counterpart in the reference: it exists for callers that cannot
+ * let the library call cudaMalloc/cudaFree -- programs whose own pool allocator holds
+ * nearly all device memory, and latency-sensitive callers that cannot absorb the
+ * device-wide wait of cudaFree when orkan_cu_exp_diag grows its scratch buffer.
+ * The per-index phase table lives in a fixed device array of 65536 entries (1 MiB per
+ * device, kept until the library is unloaded): n > 16 is rejected with a message on
+ * stderr and cudaErrorInvalidValue.  data and diag are caller-owned device buffers.  The
+ * first call on a device resolves the array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  All calls on a device share the array
+ * and it keeps the last call's contents; calls whose kernels overlap on the GPU race.
+ * Same results as orkan_cu_exp_diag; t == 0 is a no-op. */
+int orkan_cu_exp_diag_noalloc(int layout, unsigned log_tile, void *data, unsigned n, const double *diag,
+                              double t, void *stream);
+
 /* Number of kernels this library has launched in this process (all devices). */
 unsigned long long orkan_cu_launch_count(void);
 
