@@ -110,6 +110,11 @@ int orkan_cu_matel_diag(const void *bra, const void *ket, unsigned n, const doub
 int orkan_cu_exp_diag_noalloc(int layout, unsigned log_tile, void *data, unsigned n, const double *diag,
                               double t, void *stream);
 
+/* Error word of the density-matrix engine on the current device: 0, or bit 0 set when a
+ * kernel's bounded wait for staged data ran out (the kernel then stopped early instead of
+ * waiting forever).  Reads device memory, so it synchronises with the device. */
+unsigned orkan_cu_engine_status(void);
+
 /* Number of kernels this library has launched in this process (all devices). */
 unsigned long long orkan_cu_launch_count(void);
 

@@ -103,28 +103,46 @@ inline bool dm_geometry(unsigned n, unsigned k, const unsigned* qubits, unsigned
 // Sub-tile classes of position (a, b) of an item.
 enum : int { kSubDirect = 0, kSubDiag = 1, kSubTransposed = 2, kSubSkip = 3 };
 
-// Per-position descriptor of an item, built once per item in shared memory so that each
-// element's storage index, shared-memory slot(s) and skip test cost a few integer ops.
-// A "line" is a run of S consecutive storage elements of a stored sub-tile (a column
-// segment of the packed layout, a row segment of a tile); p is the offset along it.
+// ---------------------------------------------------------------------------------
+// Staging.  The block is held in shared memory as vb[M * P + m] with M the "major" and
+// m the "minor" virtual index: major = row for the tiled layout and column for the packed
+// layout, so that a line of a stored sub-tile (a tile row / a packed column segment: S
+// consecutive storage elements) lands on consecutive shared-memory addresses and moves
+// with ONE bulk copy (TMA, cp.async.bulk).  For the packed layout the block therefore
+// holds rho^T, and the gate parameters are transformed once on the host so that the same
+// group operations compute (U rho U^dagger)^T = conj(U) rho^T conj(U)^dagger
+// (dm_orient_* below).
+//
+// Region of position (a, b): major indices MB..MB+S, minor indices mB..mB+S; stored line
+// `line`, offset p lands at (MB + line) * P + mB + p.  Regions needing more than a copy:
+//   transposed position  its stored partner lands in stored orientation and is
+//                        conjugate-transposed in place after the copy (and back before
+//                        the store);
+//   diagonal sub-tile    only the stored (lower) half lands; the other half is the
+//                        conjugate transpose (for the tiled layout it is regenerated
+//                        from the lower half again before the store, so diagonal tiles
+//                        keep an exact mirror);
+//   direct position of a diagonal item (has_c)
+//                        its transposed position (b, a) is filled with the conjugate
+//                        transpose of the region.
+// ---------------------------------------------------------------------------------
 struct DmPos {
-    idx_t gbase;   // storage index of element (line 0, p 0) of the stored sub-tile
-    idx_t mbase;   // tiled: storage index of the mirror of (line 0, p 0); written at mbase + p*T + line
-    idx_t gcol;    // packed: d - PC - 1, the column-start increment per line
-    int d0, dl, dp;  // direct shared-memory slot: d0 + line*dl + p*dp
-    int c0, cl, cp;  // conjugated shared-memory slot
-    int fconst;      // virtual index constant along a line is fconst + line
-    int fvar;        // virtual index varying along a line is fvar + p
+    idx_t gbase;     // storage index of element (line 0, p 0) of the stored sub-tile
+    idx_t mbase;     // tiled: storage index of the mirror of (line 0, p 0); written at mbase + p*T + line
+    idx_t gcol;      // packed: d - PC - 1, the column-start increment per line
+    int MB, mB;      // region origin in vb (major, minor)
     int cls;         // kSub*
-    int has_c;       // a direct sub-tile that also fills its transposed position (diagonal item)
-    int mirror;      // tiled: the stored sub-tile lies in a diagonal tile; rewrite its mirror
+    int has_c;       // direct sub-tile of a diagonal item: also fill the transposed region
+    int mirror;      // tiled: the stored sub-tile lies in a diagonal tile, rewrite its mirror
+    int fconst;      // virtual index constant along a line: fconst + line
+    int fvar;        // virtual index varying along a line: fvar + p
+    int allvar;      // every fvar + p (p < S) is a fixed row/column of the gate
+    unsigned bytes;  // bytes this position's lines bring in (for the transaction count)
     int pad_;
 };
 constexpr unsigned kDmMaxPos = 64;                     // 4^h with h <= 3
 constexpr unsigned kDmPosBytes = kDmMaxPos * sizeof(DmPos);
-
-// Shared memory of one block: descriptors, then the V x (V + 1) staged block.
-ORKAN_HD size_t dm_smem_bytes(const DmGeom& g) { return kDmPosBytes + (size_t)g.V() * g.P() * 16; }
+static_assert(kDmPosBytes % 16 == 0, "descriptor block keeps the staged block 16-byte aligned");
 
 // Virtual-index bit masks of fixed rows/columns (monomial gates): bit x set when local(x)
 // is left in place with phase 1.  V <= 64, so one 64-bit word.
@@ -137,68 +155,86 @@ inline unsigned long long dm_fixed_rows(const DmGeom& g) {
     return m;
 }
 
+// Line range [p0, p1) a stored line contributes (the lower half only on diagonal sub-tiles).
+template <class Map>
+ORKAN_HD void dm_line_range(const DmPos& q, unsigned line, unsigned S, unsigned* p0, unsigned* p1) {
+    if (q.cls == kSubDiag) {
+        if (Map::kRowContig) { *p0 = line; *p1 = S; }     // packed column: rows >= column
+        else { *p0 = 0; *p1 = line + 1; }                  // tile row: columns <= row
+    } else {
+        *p0 = 0;
+        *p1 = S;
+    }
+}
+
+// A line every element of which the gate leaves in place: neither loaded nor stored.
+ORKAN_HD bool dm_line_skipped(unsigned long long fm, const DmPos& q, unsigned line) {
+    return fm && q.allvar && ((fm >> (q.fconst + line)) & 1ull);
+}
+
 // Build the descriptors of item w (threads tid < 4^h, one position each).
 template <class Map>
 ORKAN_HD void dm_setup(const Map& map, const DmGeom& g, idx_t w, DmPos* pd, unsigned tid, unsigned nthr) {
-    const unsigned h = g.h, ls = g.ls, S = g.S(), P = g.P();
+    const unsigned h = g.h, ls = g.ls, S = g.S();
     const unsigned npos = 1u << (2 * h);
     if (tid >= npos) return;
     idx_t u, v;
     tri_unrank(w, &u, &v);
     const bool diag_item = (u == v);
     const idx_t rb = insert0_sorted(u, g.hb, h), cb = insert0_sorted(v, g.hb, h);
+    const unsigned long long fm = g.fixrows;
+    const unsigned long long smask = (S >= 64) ? ~0ull : ((1ull << S) - 1ull);
     for (unsigned t = tid; t < npos; t += nthr) {
         const unsigned a = t >> h, b = t & ((1u << h) - 1);
         const idx_t R = (rb | spread_bits(a, g.hb, h)) << ls;
         const idx_t C = (cb | spread_bits(b, g.hb, h)) << ls;
+        const int aS = (int)(a * S), bS = (int)(b * S);
         DmPos q;
+        q.gbase = 0;
         q.mbase = 0;
         q.gcol = 0;
         q.has_c = 0;
         q.mirror = 0;
         q.pad_ = 0;
-        q.d0 = q.dl = q.dp = q.c0 = q.cl = q.cp = 0;
-        q.fconst = q.fvar = 0;
-        const int aS = (int)(a * S), bS = (int)(b * S);
+        q.MB = Map::kRowContig ? bS : aS;
+        q.mB = Map::kRowContig ? aS : bS;
+        // virtual coordinates along a stored line: tiled line = virtual row (aS + line) for a
+        // direct sub-tile; packed line = virtual column (bS + line); transposed: swapped
+        const bool tr = (R < C);
+        if (Map::kRowContig) { q.fconst = tr ? aS : bS; q.fvar = tr ? bS : aS; }
+        else                 { q.fconst = tr ? bS : aS; q.fvar = tr ? aS : bS; }
         if (R > C) {
             q.cls = kSubDirect;
             q.gbase = map.at(R, C);
             q.has_c = diag_item ? 1 : 0;
-            if (Map::kRowContig) {       // packed: line = column j, p = row i
-                q.d0 = aS * (int)P + bS; q.dl = 1; q.dp = (int)P;
-                q.c0 = bS * (int)P + aS; q.cl = (int)P; q.cp = 1;
-                q.fconst = bS; q.fvar = aS;
-                q.gcol = map.d - C - 1;
-            } else {                     // tiled: line = row i, p = column j
-                q.d0 = aS * (int)P + bS; q.dl = (int)P; q.dp = 1;
-                q.c0 = bS * (int)P + aS; q.cl = 1; q.cp = (int)P;
-                q.fconst = aS; q.fvar = bS;
-                if (map.same_storage_block(R, C)) { q.mirror = 1; q.mbase = map.at(C, R); }
-            }
+            if (Map::kRowContig) q.gcol = map.d - C - 1;
+            else if (map.same_storage_block(R, C)) { q.mirror = 1; q.mbase = map.at(C, R); }
         } else if (R == C) {
             q.cls = kSubDiag;
             q.gbase = map.at(R, R);
-            q.d0 = aS * (int)P + aS;
-            q.c0 = aS * (int)P + aS;
-            q.fconst = aS; q.fvar = aS;
-            if (Map::kRowContig) { q.dl = 1; q.dp = (int)P; q.cl = (int)P; q.cp = 1; q.gcol = map.d - R - 1; }
-            else                 { q.dl = (int)P; q.dp = 1; q.cl = 1; q.cp = (int)P; }
+            if (Map::kRowContig) q.gcol = map.d - R - 1;
         } else if (!diag_item) {
             q.cls = kSubTransposed;
-            q.gbase = map.at(C, R);      // stored partner (C, R)
-            if (Map::kRowContig) {       // stored (C + p, R + line) is virtual (aS + line, bS + p), conjugated
-                q.c0 = aS * (int)P + bS; q.cl = (int)P; q.cp = 1;
-                q.fconst = aS; q.fvar = bS;
-                q.gcol = map.d - R - 1;
-            } else {                     // stored (C + line, R + p) is virtual (aS + p, bS + line), conjugated
-                q.c0 = aS * (int)P + bS; q.cl = 1; q.cp = (int)P;
-                q.fconst = bS; q.fvar = aS;
-                if (map.same_storage_block(C, R)) { q.mirror = 1; q.mbase = map.at(R, C); }
-            }
+            q.gbase = map.at(C, R);                          // stored partner (C, R)
+            if (Map::kRowContig) q.gcol = map.d - R - 1;
+            else if (map.same_storage_block(C, R)) { q.mirror = 1; q.mbase = map.at(R, C); }
         } else {
             q.cls = kSubSkip;
-            q.gbase = 0;
         }
+        // tiled diagonal sub-tiles are stored as whole rows whose upper half is rebuilt from
+        // the lower half, so none of their rows may be skipped
+        const bool no_skip = Map::kMirrors && q.cls == kSubDiag;
+        q.allvar = (fm && !no_skip && ((fm >> q.fvar) & smask) == smask) ? 1 : 0;
+        unsigned bytes = 0;
+        if (q.cls != kSubSkip) {
+            for (unsigned line = 0; line < S; ++line) {
+                if (dm_line_skipped(fm, q, line)) continue;
+                unsigned p0, p1;
+                dm_line_range<Map>(q, line, S, &p0, &p1);
+                bytes += (p1 - p0) * 16u;
+            }
+        }
+        q.bytes = bytes;
         pd[t] = q;
     }
 }
@@ -210,94 +246,90 @@ ORKAN_HD idx_t dm_addr(const Map& map, const DmPos& q, unsigned line, unsigned p
     return q.gbase + ((idx_t)line << map.log_tdim()) + p;
 }
 
-ORKAN_HD bool dm_skip(unsigned long long fm, const DmPos& q, unsigned line, unsigned p) {
-    return fm && ((fm >> (q.fconst + line)) & (fm >> (q.fvar + p)) & 1ull);
-}
-
-// Load rules: which of the element's slots the load fills (bit 0 direct, bit 1 conjugate).
-template <class Map>
-ORKAN_HD unsigned dm_load_slots(const DmPos& q, unsigned line, unsigned p) {
-    switch (q.cls) {
-        case kSubDirect: return 1u | (q.has_c ? 2u : 0u);
-        case kSubTransposed: return 2u;
-        case kSubDiag:
-            if (Map::kRowContig) return p >= line ? (1u | (p > line ? 2u : 0u)) : 0u;
-            return p <= line ? (1u | (p < line ? 2u : 0u)) : 0u;
-        default: return 0u;
-    }
-}
-
-// Stage one item into the shared block vb (pitch P) with asynchronous 16-byte global->shared
-// copies (cp.async): no register staging, so a block keeps a whole item in flight while it
-// computes and stores the previous one.  An element that must also appear conjugated
-// (upper half of a diagonal sub-tile, the transposed copy of a sub-tile of a diagonal
-// item, every element of a transposed sub-tile) is copied raw into its conjugate slot and
-// fixed up by the same thread after its copies have landed (dm_fixup).
+// Bulk copies of one item: lines are numbered t = pos * S + line over all positions; the
+// caller's threads take lines tid, tid + nthr, ...  Mem::bulk_load / bulk_store move
+// (p1 - p0) consecutive elements.
 template <class Map, class Mem>
-ORKAN_HD void dm_issue(const Mem& mem, const Map& map, const DmGeom& g, const DmPos* pd, double2* vb,
-                       unsigned tid, unsigned nthr) {
-    const unsigned ls = g.ls, S = g.S();
-    const unsigned total = 1u << (2 * (ls + g.h));
-    const unsigned long long fm = g.fixrows;
-    for (unsigned f = tid; f < total; f += nthr) {
-        const DmPos& q = pd[f >> (2 * ls)];
-        const unsigned e = f & ((1u << (2 * ls)) - 1), line = e >> ls, p = e & (S - 1);
-        const unsigned which = dm_load_slots<Map>(q, line, p);
-        if (!which || dm_skip(fm, q, line, p)) continue;
-        const idx_t a = dm_addr(map, q, line, p);
-        if (which & 1u) mem.cp(vb + (q.d0 + (int)line * q.dl + (int)p * q.dp), a);
-        if (which & 2u) mem.cp(vb + (q.c0 + (int)line * q.cl + (int)p * q.cp), a);
+ORKAN_HD void dm_bulk_loads(const Mem& mem, const Map& map, const DmGeom& g, const DmPos* pd, double2* vb,
+                            void* bar, unsigned tid, unsigned nthr) {
+    const unsigned ls = g.ls, S = g.S(), P = g.P();
+    const unsigned nlines = 1u << (2 * g.h + ls);
+    for (unsigned t = tid; t < nlines; t += nthr) {
+        const DmPos& q = pd[t >> ls];
+        const unsigned line = t & (S - 1);
+        if (q.cls == kSubSkip || dm_line_skipped(g.fixrows, q, line)) continue;
+        unsigned p0, p1;
+        dm_line_range<Map>(q, line, S, &p0, &p1);
+        mem.bulk_load(vb + (q.MB + (int)line) * (int)P + q.mB + (int)p0, dm_addr(map, q, line, p0), p1 - p0, bar);
     }
 }
 
-// Conjugate the slots this thread filled through its conjugate copies (after they landed).
-template <class Map>
-ORKAN_HD void dm_fixup(const DmGeom& g, const DmPos* pd, double2* vb, unsigned tid, unsigned nthr) {
-    const unsigned ls = g.ls, S = g.S();
-    const unsigned total = 1u << (2 * (ls + g.h));
-    const unsigned long long fm = g.fixrows;
-    for (unsigned f = tid; f < total; f += nthr) {
-        const DmPos& q = pd[f >> (2 * ls)];
-        const unsigned e = f & ((1u << (2 * ls)) - 1), line = e >> ls, p = e & (S - 1);
-        if (!(dm_load_slots<Map>(q, line, p) & 2u) || dm_skip(fm, q, line, p)) continue;
-        double2& x = vb[q.c0 + (int)line * q.cl + (int)p * q.cp];
-        x.y = -x.y;
-    }
-}
-
-// Write one item back, regenerating tiled mirrors and the upper half of diagonal tiles.
 template <class Map, class Mem>
-ORKAN_HD void dm_store(const Mem& mem, const Map& map, const DmGeom& g, const DmPos* pd, const double2* vb,
-                       unsigned tid, unsigned nthr) {
-    const unsigned ls = g.ls, S = g.S();
-    const unsigned total = 1u << (2 * (ls + g.h));
-    const unsigned long long fm = g.fixrows;
+ORKAN_HD void dm_bulk_stores(const Mem& mem, const Map& map, const DmGeom& g, const DmPos* pd, const double2* vb,
+                             unsigned tid, unsigned nthr) {
+    const unsigned ls = g.ls, S = g.S(), P = g.P();
+    const unsigned nlines = 1u << (2 * g.h + ls);
+    for (unsigned t = tid; t < nlines; t += nthr) {
+        const DmPos& q = pd[t >> ls];
+        const unsigned line = t & (S - 1);
+        if (q.cls == kSubSkip || dm_line_skipped(g.fixrows, q, line)) continue;
+        unsigned p0 = 0, p1 = S;                            // tiled diagonal tiles: whole rows
+        if (Map::kRowContig) dm_line_range<Map>(q, line, S, &p0, &p1);
+        mem.bulk_store(dm_addr(map, q, line, p0), vb + (q.MB + (int)line) * (int)P + q.mB + (int)p0, p1 - p0);
+    }
+}
+
+// Tiled layout, sub-tiles smaller than a tile inside a diagonal tile: the mirror image of a
+// stored element (line, p) is at mbase + p*T + line and holds its conjugate (per element,
+// strided; occurs only when S < tile side).
+template <class Map, class Mem>
+ORKAN_HD void dm_mirror_stores(const Mem& mem, const Map& map, const DmGeom& g, const DmPos* pd,
+                               const double2* vb, unsigned tid, unsigned nthr) {
+    if (!Map::kMirrors) return;
+    const unsigned ls = g.ls, S = g.S(), P = g.P();
+    const unsigned total = 1u << (2 * (g.h + ls));
     for (unsigned f = tid; f < total; f += nthr) {
         const DmPos& q = pd[f >> (2 * ls)];
-        if (q.cls == kSubSkip) continue;
+        if (!q.mirror) continue;
         const unsigned e = f & ((1u << (2 * ls)) - 1), line = e >> ls, p = e & (S - 1);
-        if (dm_skip(fm, q, line, p)) continue;
-        double2 val;
-        if (q.cls == kSubDirect) {
-            val = vb[q.d0 + (int)line * q.dl + (int)p * q.dp];
-        } else if (q.cls == kSubTransposed) {
-            val = cconj(vb[q.c0 + (int)line * q.cl + (int)p * q.cp]);
-        } else if (Map::kRowContig) {                   // packed diagonal sub-tile: lower half only
-            if (p < line) continue;
-            val = vb[q.d0 + (int)line * q.dl + (int)p * q.dp];
-        } else {                                        // tiled diagonal sub-tile: both halves
-            val = p <= line ? vb[q.d0 + (int)line * q.dl + (int)p * q.dp]
-                            : cconj(vb[q.c0 + (int)line * q.cl + (int)p * q.cp]);
+        if (dm_line_skipped(g.fixrows, q, line)) continue;
+        mem.st(q.mbase + ((idx_t)p << map.log_tdim()) + line, cconj(vb[(q.MB + (int)line) * (int)P + q.mB + (int)p]));
+    }
+}
+
+// In-place region fix-ups (pairs (x, y) of a region handled by one thread each).
+// kind 0: after the copies land;  kind 1: before the store.
+template <class Map>
+ORKAN_HD void dm_fixups(const DmGeom& g, const DmPos* pd, double2* vb, int kind, unsigned tid, unsigned nthr) {
+    const unsigned ls = g.ls, S = g.S(), P = g.P();
+    const unsigned total = 1u << (2 * (g.h + ls));
+    for (unsigned f = tid; f < total; f += nthr) {
+        const DmPos& q = pd[f >> (2 * ls)];
+        const unsigned e = f & ((1u << (2 * ls)) - 1), x = e >> ls, y = e & (S - 1);
+        double2* r = vb + q.MB * (int)P + q.mB;
+        if (q.cls == kSubTransposed) {
+            // conjugate transpose in place: (x, y) <-> (y, x)
+            if (x > y) continue;
+            const double2 a = r[x * P + y];
+            if (x == y) { r[x * P + y] = cconj(a); continue; }
+            const double2 b = r[y * P + x];
+            r[x * P + y] = cconj(b);
+            r[y * P + x] = cconj(a);
+        } else if (q.cls == kSubDiag) {
+            if (kind == 1 && Map::kRowContig) continue;      // packed stores the lower half only
+            // fill the half that was not copied from the half that was
+            const bool landed = Map::kRowContig ? (y >= x) : (y <= x);
+            if (!landed) r[x * P + y] = cconj(r[y * P + x]);
+        } else if (q.cls == kSubDirect && q.has_c && kind == 0) {
+            // the transposed position's region: major mB.., minor MB..
+            vb[(q.mB + (int)y) * (int)P + q.MB + (int)x] = cconj(r[x * P + y]);
         }
-        mem.st(dm_addr(map, q, line, p), val);
-        if (Map::kMirrors && q.mirror)
-            mem.st(q.mbase + ((idx_t)p << map.log_tdim()) + line, cconj(val));
     }
 }
 
 // ---------------------------------------------------------------------------------
-// Group operations on the staged block.  Each thread owns whole groups, so compute
-// needs no synchronisation between threads.
+// Group operations on the staged block (vb[M * P + m]).  Each thread owns whole groups,
+// so compute needs no synchronisation between threads.
 // ---------------------------------------------------------------------------------
 
 // Virtual index with the local-index bits of gate qubits j placed (j = 0 is the MSB).
@@ -318,10 +350,10 @@ ORKAN_HD unsigned dm_get_local(unsigned x, const unsigned* vbit, unsigned k) {
 struct OpMix1 {
     double2 u[4];
     ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
-        const unsigned V = g.V(), P = g.P(), half = V >> 1, vbq = g.vbit[0];
-        const unsigned groups = half * half;
+        const unsigned P = g.P(), lh = g.ls + g.h - 1, vbq = g.vbit[0];
+        const unsigned groups = 1u << (2 * lh);
         for (unsigned t = tid; t < groups; t += nthr) {
-            const unsigned r0 = (unsigned)insert0(t / half, vbq), c0 = (unsigned)insert0(t % half, vbq);
+            const unsigned r0 = (unsigned)insert0(t >> lh, vbq), c0 = (unsigned)insert0(t & ((1u << lh) - 1), vbq);
             const unsigned r1 = r0 | (1u << vbq), c1 = c0 | (1u << vbq);
             const double2 x00 = vb[r0 * P + c0], x01 = vb[r0 * P + c1];
             const double2 x10 = vb[r1 * P + c0], x11 = vb[r1 * P + c1];
@@ -343,13 +375,13 @@ struct OpMix1 {
 struct OpMix2 {
     double2 u[16];
     ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
-        const unsigned V = g.V(), P = g.P(), quarter = V >> 2;
+        const unsigned P = g.P(), lq = g.ls + g.h - 2;
         unsigned asc[2] = {g.vbit[0] < g.vbit[1] ? g.vbit[0] : g.vbit[1],
                            g.vbit[0] < g.vbit[1] ? g.vbit[1] : g.vbit[0]};
-        const unsigned groups = quarter * quarter;
+        const unsigned groups = 1u << (2 * lq);
         for (unsigned t = tid; t < groups; t += nthr) {
-            const unsigned rb = (unsigned)insert0_sorted(t / quarter, asc, 2);
-            const unsigned cb = (unsigned)insert0_sorted(t % quarter, asc, 2);
+            const unsigned rb = (unsigned)insert0_sorted(t >> lq, asc, 2);
+            const unsigned cb = (unsigned)insert0_sorted(t & ((1u << lq) - 1), asc, 2);
             unsigned ri[4], ci[4];
             for (unsigned l = 0; l < 4; ++l) {
                 ri[l] = dm_set_local(rb, l, g.vbit, 2);
@@ -376,10 +408,10 @@ struct OpMix2 {
 struct OpSuper1 {
     double2 s[16];
     ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
-        const unsigned V = g.V(), P = g.P(), half = V >> 1, vbq = g.vbit[0];
-        const unsigned groups = half * half;
+        const unsigned P = g.P(), lh = g.ls + g.h - 1, vbq = g.vbit[0];
+        const unsigned groups = 1u << (2 * lh);
         for (unsigned t = tid; t < groups; t += nthr) {
-            const unsigned r0 = (unsigned)insert0(t / half, vbq), c0 = (unsigned)insert0(t % half, vbq);
+            const unsigned r0 = (unsigned)insert0(t >> lh, vbq), c0 = (unsigned)insert0(t & ((1u << lh) - 1), vbq);
             const unsigned r1 = r0 | (1u << vbq), c1 = c0 | (1u << vbq);
             const unsigned idx[4] = {r0 * P + c0, r0 * P + c1, r1 * P + c0, r1 * P + c1};
             double2 x[4];
@@ -401,13 +433,13 @@ struct OpMonomial {
     unsigned src[8];
     double2 phase[8];
     ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
-        const unsigned V = g.V(), P = g.P(), k = g.k;
+        const unsigned V = g.V(), P = g.P(), k = g.k, lv = g.ls + g.h;
         const unsigned total = V * V;
         for (unsigned f = tid; f < total; f += nthr) {
-            const unsigned r = f / V, c = f % V;
+            const unsigned r = f >> lv, c = f & (V - 1);
             const unsigned lr = dm_get_local(r, g.vbit, k), lc = dm_get_local(c, g.vbit, k);
             const unsigned r2 = dm_set_local(r, src[lr], g.vbit, k), c2i = dm_set_local(c, src[lc], g.vbit, k);
-            const unsigned f2 = r2 * V + c2i;
+            const unsigned f2 = (r2 << lv) + c2i;
             if (f2 < f) continue;
             const double2 fa = cmulc(phase[lr], phase[lc]);
             if (f2 == f) {
@@ -430,67 +462,175 @@ inline unsigned monomial_fixmask(const OpMonomial& op, unsigned m) {
     return mask;
 }
 
-// One work item, phase by phase (the CPU emulator runs each phase for all threads
-// before the next; the kernel below overlaps items with a two-stage pipeline).
+// The packed layout stages rho^T: (U rho U^dagger)^T = conj(U) rho^T conj(U)^dagger, so its
+// operators are the complex conjugates; a superoperator on vec(rho_2x2) = (00, 01, 10, 11)
+// acts on vec(rho^T) with 01 and 10 exchanged in both its rows and its columns.
+inline void dm_orient(OpMix1& op, bool transposed) {
+    if (transposed) for (auto& z : op.u) z = cconj(z);
+}
+inline void dm_orient(OpMix2& op, bool transposed) {
+    if (transposed) for (auto& z : op.u) z = cconj(z);
+}
+inline void dm_orient(OpMonomial& op, bool transposed) {
+    if (transposed) for (auto& z : op.phase) z = cconj(z);
+}
+inline void dm_orient(OpSuper1& op, bool transposed) {
+    if (!transposed) return;
+    const unsigned perm[4] = {0, 2, 1, 3};
+    double2 t[16];
+    for (unsigned m = 0; m < 4; ++m)
+        for (unsigned j = 0; j < 4; ++j) t[4 * m + j] = op.s[4 * perm[m] + perm[j]];
+    for (unsigned i = 0; i < 16; ++i) op.s[i] = t[i];
+}
+
+// Shared memory of one block of the pipelined engine: two mbarriers, then two stages of
+// (descriptors, staged block).
+ORKAN_HD size_t dm_stage_bytes(const DmGeom& g) { return kDmPosBytes + (size_t)g.V() * g.P() * 16; }
+ORKAN_HD size_t dm_pipe_smem_bytes(const DmGeom& g) { return 16 + 2 * dm_stage_bytes(g); }
+
+// One work item, phase by phase (the CPU emulator runs each phase for all threads before
+// the next; the kernel below overlaps items with a two-stage pipeline).
 template <class Map, class Mem, class Op>
 ORKAN_HD void dm_engine_item_phase(int phase, const Mem& mem, const Map& map, const DmGeom& g, const Op& op,
                                    idx_t w, DmPos* pd, double2* vb, unsigned tid, unsigned nthr) {
-    if (phase == 0) dm_setup(map, g, w, pd, tid, nthr);
-    else if (phase == 1) dm_issue(mem, map, g, pd, vb, tid, nthr);
-    else if (phase == 2) dm_fixup<Map>(g, pd, vb, tid, nthr);
-    else if (phase == 3) op(g, vb, tid, nthr);
-    else dm_store(mem, map, g, pd, vb, tid, nthr);
+    switch (phase) {
+        case 0: dm_setup(map, g, w, pd, tid, nthr); break;
+        case 1: dm_bulk_loads(mem, map, g, pd, vb, nullptr, tid, nthr); break;
+        case 2: dm_fixups<Map>(g, pd, vb, 0, tid, nthr); break;
+        case 3: op(g, vb, tid, nthr); break;
+        case 4: dm_fixups<Map>(g, pd, vb, 1, tid, nthr); break;
+        case 5: dm_bulk_stores(mem, map, g, pd, vb, tid, nthr); break;
+        default: dm_mirror_stores(mem, map, g, pd, vb, tid, nthr); break;
+    }
 }
+constexpr int kDmPhases = 7;
 
-constexpr unsigned kDmBlock = 512;          // threads of the pipelined engine block
-
-// Shared memory of one pipelined block: two descriptor sets and two staged blocks.
-ORKAN_HD size_t dm_pipe_smem_bytes(const DmGeom& g) { return 2 * dm_smem_bytes(g); }
+constexpr unsigned kDmBlock = 256;          // threads of the pipelined engine block
+constexpr unsigned kDmIssueThreads = 64;    // threads that issue the bulk copies
 
 #ifdef __CUDACC__
-struct DevMemAsync : DevMem {
-    __device__ __forceinline__ void cp(double2* sdst, idx_t i) const {
-        const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(p + i) : "memory");
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+struct DevMemBulk {
+    double2* p;
+    __device__ __forceinline__ void st(idx_t i, double2 v) const { p[i] = v; }
+    __device__ __forceinline__ void bulk_load(double2* sdst, idx_t i, unsigned n, void* bar) const {
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                     ::"r"(smem_u32(sdst)), "l"(p + i), "r"(n * 16u), "r"(smem_u32(bar)) : "memory");
+    }
+    __device__ __forceinline__ void bulk_store(idx_t i, const double2* ssrc, unsigned n) const {
+        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n"
+                     ::"l"(p + i), "r"(smem_u32(ssrc)), "r"(n * 16u) : "memory");
     }
 };
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Persistent, double-buffered engine: block b handles items b, b + G, b + 2G, ...; the
-// copies of the next item are in flight while the current one is computed and stored.
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+
+// Error word of the engine: bit 0 set when a wait for staged data ran past its limit.
+__device__ unsigned int g_dm_engine_error;
+constexpr unsigned long long kDmWaitLimit = 1ull << 24;
+
+// Bounded wait for the copies of a stage (false: limit reached, error recorded).
+__device__ __forceinline__ bool dm_wait_stage(unsigned long long* bar, unsigned parity) {
+    for (unsigned long long i = 0; i < kDmWaitLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicOr(&g_dm_engine_error, 1u);
+    return false;
+}
+
+// Persistent, double-buffered engine: block b handles items b, b + G, b + 2G, ...; the bulk
+// copies of the next item are in flight while the current one is fixed up, computed and
+// stored.  The staged block is read back to global memory with bulk stores.
 template <class Map, class Op>
-__global__ void __launch_bounds__(kDmBlock) k_dm_engine(DevMemAsync mem, Map map, DmGeom g, Op op) {
-    extern __shared__ double2 smem[];
-    const size_t half = dm_smem_bytes(g) / sizeof(double2);
-    DmPos* pd[2] = {reinterpret_cast<DmPos*>(smem), reinterpret_cast<DmPos*>(smem + half)};
-    double2* vb[2] = {smem + kDmPosBytes / sizeof(double2), smem + half + kDmPosBytes / sizeof(double2)};
+__global__ void __launch_bounds__(kDmBlock) k_dm_engine(DevMemBulk mem, Map map, DmGeom g, Op op) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem_raw);
+    const size_t stage = dm_stage_bytes(g);
+    DmPos* pd[2] = {reinterpret_cast<DmPos*>(smem_raw + 16), reinterpret_cast<DmPos*>(smem_raw + 16 + stage)};
+    double2* vb[2] = {reinterpret_cast<double2*>(smem_raw + 16 + kDmPosBytes),
+                      reinterpret_cast<double2*>(smem_raw + 16 + stage + kDmPosBytes)};
     const unsigned tid = threadIdx.x, nthr = blockDim.x;
+    const unsigned npos = 1u << (2 * g.h);
     idx_t w = blockIdx.x;
     if (w >= g.items) return;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
     dm_setup(map, g, w, pd[0], tid, nthr);
     __syncthreads();
-    dm_issue(mem, map, g, pd[0], vb[0], tid, nthr);
-    cp_commit();
+    unsigned parity[2] = {0u, 0u};
+    if (tid == 0) {
+        unsigned bytes = 0;
+        for (unsigned t = 0; t < npos; ++t) bytes += pd[0][t].bytes;
+        mbar_arrive_expect(&bars[0], bytes);
+    }
+    __syncthreads();
+    if (tid < kDmIssueThreads) dm_bulk_loads(mem, map, g, pd[0], vb[0], &bars[0], tid, kDmIssueThreads);
+    bool ok = true;
     for (unsigned it = 0;; ++it) {
         const unsigned cur = it & 1u, nxt = cur ^ 1u;
         const idx_t wn = w + gridDim.x;
-        if (wn < g.items) dm_setup(map, g, wn, pd[nxt], tid, nthr);
-        __syncthreads();                                  // pd[nxt] ready; vb[nxt] free
-        if (wn < g.items) dm_issue(mem, map, g, pd[nxt], vb[nxt], tid, nthr);
-        cp_commit();
-        cp_wait<1>();                                     // this thread's copies of item w landed
-        dm_fixup<Map>(g, pd[cur], vb[cur], tid, nthr);
+        const bool more = wn < g.items;
+        if (more) dm_setup(map, g, wn, pd[nxt], tid, nthr);
+        __syncthreads();                                    // pd[nxt] ready; vb[nxt] no longer read
+        if (more) {
+            if (tid == 0) {
+                unsigned bytes = 0;
+                for (unsigned t = 0; t < npos; ++t) bytes += pd[nxt][t].bytes;
+                mbar_arrive_expect(&bars[nxt], bytes);
+            }
+            __syncthreads();
+            if (tid < kDmIssueThreads) {
+                fence_proxy_async();
+                dm_bulk_loads(mem, map, g, pd[nxt], vb[nxt], &bars[nxt], tid, kDmIssueThreads);
+            }
+        }
+        ok = __syncthreads_and(dm_wait_stage(&bars[cur], parity[cur]) ? 1 : 0) != 0;
+        parity[cur] ^= 1u;
+        if (!ok) break;
+        dm_fixups<Map>(g, pd[cur], vb[cur], 0, tid, nthr);
         __syncthreads();
         op(g, vb[cur], tid, nthr);
         __syncthreads();
-        dm_store(mem, map, g, pd[cur], vb[cur], tid, nthr);
-        if (wn >= g.items) break;
+        dm_fixups<Map>(g, pd[cur], vb[cur], 1, tid, nthr);
+        fence_proxy_async();
+        __syncthreads();
+        if (tid < kDmIssueThreads) {
+            dm_bulk_stores(mem, map, g, pd[cur], vb[cur], tid, kDmIssueThreads);
+            bulk_commit();
+        }
+        dm_mirror_stores(mem, map, g, pd[cur], vb[cur], tid, nthr);
+        if (tid < kDmIssueThreads) bulk_wait_read();          // staged block free again
+        if (!more) break;
         w = wn;
-        __syncthreads();                                  // vb[cur], pd[cur] free for item w + 2G
     }
-    cp_wait<0>();
+    if (!ok) {
+        // give the copies still in flight for the other stage a bounded chance to land
+        for (unsigned s = 0; s < 2; ++s)
+            for (unsigned long long i = 0; i < kDmWaitLimit && !mbar_try_wait(&bars[s], parity[s]); ++i) {
+            }
+    }
+    if (tid < kDmIssueThreads) bulk_wait_all();
 }
 #endif
 

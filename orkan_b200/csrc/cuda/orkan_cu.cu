@@ -54,7 +54,7 @@ template <class Kern>
 unsigned engine_grid(Kern kern, size_t smem, idx_t items) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * (int)(kDmPosBytes + 64 * 65 * 16));
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         attr = true;
     }
     int per_sm = 0;
@@ -64,11 +64,11 @@ unsigned engine_grid(Kern kern, size_t smem, idx_t items) {
 }
 
 template <class Op>
-int launch_engine_map(int layout, unsigned log_tile, void* rho, unsigned n, const DmGeom& g, const Op& op,
+int launch_engine_map(int layout, unsigned log_tile, void* rho, unsigned n, const DmGeom& g, Op op,
                       cudaStream_t st) {
     const size_t smem = dm_pipe_smem_bytes(g);
-    DevMemAsync mem;
-    mem.p = static_cast<double2*>(rho);
+    dm_orient(op, layout == 1);               // the packed layout stages rho^T
+    DevMemBulk mem{static_cast<double2*>(rho)};
     if (layout == 1) {
         auto kern = k_dm_engine<PackedMap, Op>;
         const unsigned grid = engine_grid(kern, smem, g.items);
@@ -328,5 +328,12 @@ int orkan_cu_matel_diag(const void* bra, const void* ket, unsigned n, const doub
 }
 
 unsigned long long orkan_cu_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+// Error word of the density-matrix engine (non-zero: a wait for staged data ran out).
+unsigned orkan_cu_engine_status(void) {
+    unsigned v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_dm_engine_error, sizeof(v)) != cudaSuccess) return 0xffffffffu;
+    return v;
+}
 
 }  // extern "C"

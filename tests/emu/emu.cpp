@@ -46,6 +46,13 @@ struct EmuMem {
         *dst = p[i];
     }
     mutable idx_t last_cp = ~idx_t(0);
+    // bulk copies of the GPU path (TMA): n consecutive elements, land immediately here
+    void bulk_load(double2* sdst, idx_t i, unsigned n, void*) const {
+        for (unsigned k = 0; k < n; ++k) sdst[k] = ld(i + k);
+    }
+    void bulk_store(idx_t i, const double2* ssrc, unsigned n) const {
+        for (unsigned k = 0; k < n; ++k) st(i + k, ssrc[k]);
+    }
 };
 
 struct EmuMemR {
@@ -84,11 +91,15 @@ void run_engine(const EmuMem& mem, const Map& map, const DmGeom& g, const Op& op
     const unsigned grid = grid_for(1, g.items, kSms * 32u);
     std::vector<double2> vb((size_t)g.V() * g.P());
     std::vector<DmPos> pd(kDmMaxPos);
+    Op o = op;
+    dm_orient(o, !Map::kMirrors);           // the packed layout stages rho^T
     for (unsigned b = 0; b < grid; ++b) {
         for (idx_t w = b; w < g.items; w += grid) {
-            for (int phase = 0; phase < 5; ++phase)
-                for (unsigned t = 0; t < kDmBlock; ++t)
-                    dm_engine_item_phase(phase, mem, map, g, op, w, pd.data(), vb.data(), t, kDmBlock);
+            for (int phase = 0; phase < kDmPhases; ++phase) {
+                const unsigned nthr = (phase == 1 || phase == 5) ? kDmIssueThreads : kDmBlock;
+                for (unsigned t = 0; t < nthr; ++t)
+                    dm_engine_item_phase(phase, mem, map, g, o, w, pd.data(), vb.data(), t, nthr);
+            }
         }
     }
 }

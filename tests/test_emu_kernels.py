@@ -40,8 +40,10 @@ def storage_rc(kind, n, lt):
 
 def check_engine_counts(kind, n, lt, res, gate=None, qubits=None):
     """Every stored lower-triangle element the gate may change is read once and written
-    once; the tiled diagonal-tile mirrors are written once, never read; elements the gate
-    leaves in place (monomial gates) and the tiled padding are not touched at all."""
+    once; the tiled diagonal-tile mirrors are never read and are written once when they
+    may change; elements a monomial gate leaves in place are read and written at most once
+    (whole lines of them are skipped; the oracle comparison checks their values); the tiled
+    padding is never touched."""
     r, c, live = storage_rc(kind, n, lt)
     assert res.oob == 0
     changed = np.ones(r.shape, dtype=bool)
@@ -53,7 +55,7 @@ def check_engine_counts(kind, n, lt, res, gate=None, qubits=None):
     assert np.all(res.writes[lower & changed] == 1)
     assert np.all(res.reads[upper] == 0)
     assert np.all(res.writes[upper & changed] == 1)
-    assert np.all(res.reads[~changed] == 0) and np.all(res.writes[~changed] == 0)
+    assert res.reads.max(initial=0) <= 1 and res.writes.max(initial=0) <= 1
     assert np.all(res.reads[~live] == 0) and np.all(res.writes[~live] == 0)
 
 

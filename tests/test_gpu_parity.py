@@ -279,3 +279,11 @@ def test_full_size_mixed_14q_properties(ork5, kind):
         ork5.gate(st, inv.get(g, g), qs, -th if th is not None else None)
     assert np.abs(ork5.storage(st) - start).max() <= 1e-12
     ork5.free(st)
+
+
+def test_engine_reported_no_errors(ork5, ork3):
+    """No density-matrix engine launch of this process ran out of its bounded wait for staged
+    data (the kernel records that in an error word instead of waiting forever)."""
+    for ork in (ork5, ork3):
+        ork.lib.orkan_cu_engine_status.restype = __import__("ctypes").c_uint
+        assert ork.lib.orkan_cu_engine_status() == 0
