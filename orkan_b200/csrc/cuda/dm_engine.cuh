@@ -279,50 +279,82 @@ ORKAN_HD void dm_bulk_stores(const Mem& mem, const Map& map, const DmGeom& g, co
     }
 }
 
+// Does position q need work in pass `kind` (0: after the copies land, 1: before the store,
+// 2: per-element mirror stores)?
+template <class Map>
+ORKAN_HD bool dm_needs(const DmPos& q, int kind) {
+    if (kind == 2) return Map::kMirrors && q.mirror;
+    if (q.cls == kSubTransposed) return true;
+    if (q.cls == kSubDiag) return kind == 0 || Map::kMirrors;
+    return kind == 0 && q.cls == kSubDirect && q.has_c;
+}
+
+// Bit mask over the item's positions of those needing pass `kind`.
+template <class Map>
+ORKAN_HD unsigned long long dm_pass_mask(const DmPos* pd, unsigned npos, int kind) {
+#ifdef __CUDA_ARCH__
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lo = __ballot_sync(0xffffffffu, lane < npos && dm_needs<Map>(pd[lane], kind));
+    const unsigned hi = __ballot_sync(0xffffffffu, lane + 32 < npos && dm_needs<Map>(pd[lane + 32], kind));
+    return (unsigned long long)lo | ((unsigned long long)hi << 32);
+#else
+    unsigned long long m = 0;
+    for (unsigned t = 0; t < npos; ++t)
+        if (dm_needs<Map>(pd[t], kind)) m |= 1ull << t;
+    return m;
+#endif
+}
+
 // Tiled layout, sub-tiles smaller than a tile inside a diagonal tile: the mirror image of a
 // stored element (line, p) is at mbase + p*T + line and holds its conjugate (per element,
 // strided; occurs only when S < tile side).
 template <class Map, class Mem>
 ORKAN_HD void dm_mirror_stores(const Mem& mem, const Map& map, const DmGeom& g, const DmPos* pd,
-                               const double2* vb, unsigned tid, unsigned nthr) {
+                               const double2* vb, unsigned long long mask, unsigned tid, unsigned nthr) {
     if (!Map::kMirrors) return;
     const unsigned ls = g.ls, S = g.S(), P = g.P();
-    const unsigned total = 1u << (2 * (g.h + ls));
-    for (unsigned f = tid; f < total; f += nthr) {
-        const DmPos& q = pd[f >> (2 * ls)];
-        if (!q.mirror) continue;
-        const unsigned e = f & ((1u << (2 * ls)) - 1), line = e >> ls, p = e & (S - 1);
-        if (dm_line_skipped(g.fixrows, q, line)) continue;
-        mem.st(q.mbase + ((idx_t)p << map.log_tdim()) + line, cconj(vb[(q.MB + (int)line) * (int)P + q.mB + (int)p]));
+    while (mask) {
+        const unsigned t = (unsigned)__builtin_ctzll(mask);
+        mask &= mask - 1;
+        const DmPos& q = pd[t];
+        for (unsigned e = tid; e < (1u << (2 * ls)); e += nthr) {
+            const unsigned line = e >> ls, p = e & (S - 1);
+            if (dm_line_skipped(g.fixrows, q, line)) continue;
+            mem.st(q.mbase + ((idx_t)p << map.log_tdim()) + line,
+                   cconj(vb[(q.MB + (int)line) * (int)P + q.mB + (int)p]));
+        }
     }
 }
 
-// In-place region fix-ups (pairs (x, y) of a region handled by one thread each).
-// kind 0: after the copies land;  kind 1: before the store.
+// In-place region fix-ups of the positions in `mask` (pairs (x, y) of a region handled by
+// one thread each).  kind 0: after the copies land;  kind 1: before the store.
 template <class Map>
-ORKAN_HD void dm_fixups(const DmGeom& g, const DmPos* pd, double2* vb, int kind, unsigned tid, unsigned nthr) {
+ORKAN_HD void dm_fixups(const DmGeom& g, const DmPos* pd, double2* vb, int kind, unsigned long long mask,
+                        unsigned tid, unsigned nthr) {
     const unsigned ls = g.ls, S = g.S(), P = g.P();
-    const unsigned total = 1u << (2 * (g.h + ls));
-    for (unsigned f = tid; f < total; f += nthr) {
-        const DmPos& q = pd[f >> (2 * ls)];
-        const unsigned e = f & ((1u << (2 * ls)) - 1), x = e >> ls, y = e & (S - 1);
+    while (mask) {
+        const unsigned t = (unsigned)__builtin_ctzll(mask);
+        mask &= mask - 1;
+        const DmPos& q = pd[t];
         double2* r = vb + q.MB * (int)P + q.mB;
-        if (q.cls == kSubTransposed) {
-            // conjugate transpose in place: (x, y) <-> (y, x)
-            if (x > y) continue;
-            const double2 a = r[x * P + y];
-            if (x == y) { r[x * P + y] = cconj(a); continue; }
-            const double2 b = r[y * P + x];
-            r[x * P + y] = cconj(b);
-            r[y * P + x] = cconj(a);
-        } else if (q.cls == kSubDiag) {
-            if (kind == 1 && Map::kRowContig) continue;      // packed stores the lower half only
-            // fill the half that was not copied from the half that was
-            const bool landed = Map::kRowContig ? (y >= x) : (y <= x);
-            if (!landed) r[x * P + y] = cconj(r[y * P + x]);
-        } else if (q.cls == kSubDirect && q.has_c && kind == 0) {
-            // the transposed position's region: major mB.., minor MB..
-            vb[(q.mB + (int)y) * (int)P + q.MB + (int)x] = cconj(r[x * P + y]);
+        for (unsigned e = tid; e < (1u << (2 * ls)); e += nthr) {
+            const unsigned x = e >> ls, y = e & (S - 1);
+            if (q.cls == kSubTransposed) {
+                // conjugate transpose in place: (x, y) <-> (y, x)
+                if (x > y) continue;
+                const double2 a = r[x * P + y];
+                if (x == y) { r[x * P + y] = cconj(a); continue; }
+                const double2 b = r[y * P + x];
+                r[x * P + y] = cconj(b);
+                r[y * P + x] = cconj(a);
+            } else if (q.cls == kSubDiag) {
+                // fill the half that was not copied from the half that was
+                const bool landed = Map::kRowContig ? (y >= x) : (y <= x);
+                if (!landed) r[x * P + y] = cconj(r[y * P + x]);
+            } else {
+                // direct sub-tile of a diagonal item: its transposed position (major mB.., minor MB..)
+                vb[(q.mB + (int)y) * (int)P + q.MB + (int)x] = cconj(r[x * P + y]);
+            }
         }
     }
 }
@@ -493,19 +525,20 @@ ORKAN_HD size_t dm_pipe_smem_bytes(const DmGeom& g) { return 16 + 2 * dm_stage_b
 template <class Map, class Mem, class Op>
 ORKAN_HD void dm_engine_item_phase(int phase, const Mem& mem, const Map& map, const DmGeom& g, const Op& op,
                                    idx_t w, DmPos* pd, double2* vb, unsigned tid, unsigned nthr) {
+    const unsigned npos = 1u << (2 * g.h);
     switch (phase) {
         case 0: dm_setup(map, g, w, pd, tid, nthr); break;
         case 1: dm_bulk_loads(mem, map, g, pd, vb, nullptr, tid, nthr); break;
-        case 2: dm_fixups<Map>(g, pd, vb, 0, tid, nthr); break;
+        case 2: dm_fixups<Map>(g, pd, vb, 0, dm_pass_mask<Map>(pd, npos, 0), tid, nthr); break;
         case 3: op(g, vb, tid, nthr); break;
-        case 4: dm_fixups<Map>(g, pd, vb, 1, tid, nthr); break;
+        case 4: dm_fixups<Map>(g, pd, vb, 1, dm_pass_mask<Map>(pd, npos, 1), tid, nthr); break;
         case 5: dm_bulk_stores(mem, map, g, pd, vb, tid, nthr); break;
-        default: dm_mirror_stores(mem, map, g, pd, vb, tid, nthr); break;
+        default: dm_mirror_stores(mem, map, g, pd, vb, dm_pass_mask<Map>(pd, npos, 2), tid, nthr); break;
     }
 }
 constexpr int kDmPhases = 7;
 
-constexpr unsigned kDmBlock = 256;          // threads of the pipelined engine block
+constexpr unsigned kDmBlock = 512;          // threads of the pipelined engine block
 constexpr unsigned kDmIssueThreads = 64;    // threads that issue the bulk copies
 
 #ifdef __CUDACC__
@@ -608,18 +641,26 @@ __global__ void __launch_bounds__(kDmBlock) k_dm_engine(DevMemBulk mem, Map map,
         ok = __syncthreads_and(dm_wait_stage(&bars[cur], parity[cur]) ? 1 : 0) != 0;
         parity[cur] ^= 1u;
         if (!ok) break;
-        dm_fixups<Map>(g, pd[cur], vb[cur], 0, tid, nthr);
-        __syncthreads();
+        const unsigned long long fix0 = dm_pass_mask<Map>(pd[cur], npos, 0);
+        const unsigned long long fix1 = dm_pass_mask<Map>(pd[cur], npos, 1);
+        const unsigned long long mirr = dm_pass_mask<Map>(pd[cur], npos, 2);
+        if (fix0) {
+            dm_fixups<Map>(g, pd[cur], vb[cur], 0, fix0, tid, nthr);
+            __syncthreads();
+        }
         op(g, vb[cur], tid, nthr);
         __syncthreads();
-        dm_fixups<Map>(g, pd[cur], vb[cur], 1, tid, nthr);
+        if (fix1) {
+            dm_fixups<Map>(g, pd[cur], vb[cur], 1, fix1, tid, nthr);
+            __syncthreads();
+        }
         fence_proxy_async();
         __syncthreads();
         if (tid < kDmIssueThreads) {
             dm_bulk_stores(mem, map, g, pd[cur], vb[cur], tid, kDmIssueThreads);
             bulk_commit();
         }
-        dm_mirror_stores(mem, map, g, pd[cur], vb[cur], tid, nthr);
+        if (mirr) dm_mirror_stores(mem, map, g, pd[cur], vb[cur], mirr, tid, nthr);
         if (tid < kDmIssueThreads) bulk_wait_read();          // staged block free again
         if (!more) break;
         w = wn;
