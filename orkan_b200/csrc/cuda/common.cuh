@@ -47,6 +47,15 @@ ORKAN_HD idx_t spread_bits(unsigned a, const unsigned* p, unsigned k) {
     return r;
 }
 
+// Index of the lowest set bit of a non-zero 64-bit word.
+ORKAN_HD unsigned ctz64(unsigned long long x) {
+#ifdef __CUDA_ARCH__
+    return (unsigned)(__ffsll((long long)x) - 1);
+#else
+    return (unsigned)__builtin_ctzll(x);
+#endif
+}
+
 // Row r of the lower-triangular enumeration w = u*(u+1)/2 + v, v <= u.
 ORKAN_HD void tri_unrank(idx_t w, idx_t* u, idx_t* v) {
     idx_t uu = (idx_t)((sqrt(8.0 * (double)w + 1.0) - 1.0) * 0.5);

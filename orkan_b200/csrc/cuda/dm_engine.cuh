@@ -314,7 +314,7 @@ ORKAN_HD void dm_mirror_stores(const Mem& mem, const Map& map, const DmGeom& g, 
     if (!Map::kMirrors) return;
     const unsigned ls = g.ls, S = g.S(), P = g.P();
     while (mask) {
-        const unsigned t = (unsigned)__builtin_ctzll(mask);
+        const unsigned t = ctz64(mask);
         mask &= mask - 1;
         const DmPos& q = pd[t];
         for (unsigned e = tid; e < (1u << (2 * ls)); e += nthr) {
@@ -333,7 +333,7 @@ ORKAN_HD void dm_fixups(const DmGeom& g, const DmPos* pd, double2* vb, int kind,
                         unsigned tid, unsigned nthr) {
     const unsigned ls = g.ls, S = g.S(), P = g.P();
     while (mask) {
-        const unsigned t = (unsigned)__builtin_ctzll(mask);
+        const unsigned t = ctz64(mask);
         mask &= mask - 1;
         const DmPos& q = pd[t];
         double2* r = vb + q.MB * (int)P + q.mB;
