@@ -664,6 +664,7 @@ __global__ void __launch_bounds__(kDmBlock) k_dm_engine(DevMemBulk mem, Map map,
         if (tid < kDmIssueThreads) bulk_wait_read();          // staged block free again
         if (!more) break;
         w = wn;
+        __syncthreads();       // every thread is done with stage cur before the next setup refills it
     }
     if (!ok) {
         // give the copies still in flight for the other stage a bounded chance to land

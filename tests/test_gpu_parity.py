@@ -287,3 +287,28 @@ def test_engine_reported_no_errors(ork5, ork3):
     for ork in (ork5, ork3):
         ork.lib.orkan_cu_engine_status.restype = __import__("ctypes").c_uint
         assert ork.lib.orkan_cu_engine_status() == 0
+
+
+@pytest.mark.parametrize("kind", ["packed", "tiled"])
+def test_engine_pipeline_many_items_per_block(ork5, kind):
+    """12 q density matrices: thousands of engine work items, so every block runs its
+    double-buffered pipeline over many items (small states give each block at most one)."""
+    n = 12
+    rng = np.random.default_rng(21)
+    rho = rand_rho(n, 31)
+    st = ork5.state(kind, n, R.to_storage(kind, rho, 5))
+    seq = [("h", (0,), None), ("h", (11,), None), ("rx", (6,), 0.3), ("ry", (3,), 1.1), ("x", (9,), None),
+           ("y", (1,), None), ("cx", (11, 0), None), ("cx", (2, 10), None), ("cy", (7, 8), None),
+           ("swap", (11, 5), None), ("swap", (1, 2), None), ("ccx", (11, 10, 0), None), ("ccx", (0, 1, 9), None)]
+    for g, qs, th in seq:
+        ork5.gate(st, g, qs, th)
+        rho = R.apply_mixed(rho, g, qs, th)
+    sop = R.kraus_to_superop(R.amplitude_damping_kraus(0.3))
+    for q in (0, 7, 11):
+        ork5.channel_1q(st, sop, q)
+        rho = R.apply_superop1(rho, sop, q)
+    u, _ = np.linalg.qr(rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4)))
+    ork5.two_from_mat(st, 11, 4, u.reshape(-1, order="F"))
+    rho = R.conjugate_by(rho, u, [11, 4], n)
+    assert np.abs(ork5.storage(st) - R.to_storage(kind, rho, 5)).max() <= TOL
+    ork5.free(st)
