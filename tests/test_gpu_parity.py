@@ -281,14 +281,6 @@ def test_full_size_mixed_14q_properties(ork5, kind):
     ork5.free(st)
 
 
-def test_engine_reported_no_errors(ork5, ork3):
-    """No density-matrix engine launch of this process ran out of its bounded wait for staged
-    data (the kernel records that in an error word instead of waiting forever)."""
-    for ork in (ork5, ork3):
-        ork.lib.orkan_cu_engine_status.restype = __import__("ctypes").c_uint
-        assert ork.lib.orkan_cu_engine_status() == 0
-
-
 @pytest.mark.parametrize("kind", ["packed", "tiled"])
 def test_engine_pipeline_many_items_per_block(ork5, kind):
     """12 q density matrices: thousands of engine work items, so every block runs its
@@ -312,3 +304,12 @@ def test_engine_pipeline_many_items_per_block(ork5, kind):
     rho = R.conjugate_by(rho, u, [11, 4], n)
     assert np.abs(ork5.storage(st) - R.to_storage(kind, rho, 5)).max() <= TOL
     ork5.free(st)
+
+
+def test_engine_reported_no_errors(ork5, ork3):
+    """No density-matrix engine launch of this process ran out of its bounded wait for staged
+    data (the kernel records that in an error word instead of waiting forever)."""
+    for ork in (ork5, ork3):
+        ork.lib.orkan_cu_engine_status.restype = __import__("ctypes").c_uint
+        assert ork.lib.orkan_cu_engine_status() == 0
+
