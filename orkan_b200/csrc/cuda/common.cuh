@@ -56,6 +56,24 @@ ORKAN_HD unsigned ctz64(unsigned long long x) {
 #endif
 }
 
+ORKAN_HD unsigned popc64(unsigned long long x) {
+#ifdef __CUDA_ARCH__
+    return (unsigned)__popcll(x);
+#else
+    return (unsigned)__builtin_popcountll(x);
+#endif
+}
+
+// Row u, column v of the lower-triangular item index w = u(u+1)/2 + v: single-precision
+// estimate corrected exactly in integers.
+ORKAN_HD void tri_unrank_f(idx_t w, idx_t* u, idx_t* v) {
+    idx_t uu = (idx_t)((sqrtf(8.0f * (float)w + 1.0f) - 1.0f) * 0.5f);
+    while (uu > 0 && uu * (uu + 1) / 2 > w) --uu;
+    while ((uu + 1) * (uu + 2) / 2 <= w) ++uu;
+    *u = uu;
+    *v = w - uu * (uu + 1) / 2;
+}
+
 // Row r of the lower-triangular enumeration w = u*(u+1)/2 + v, v <= u.
 ORKAN_HD void tri_unrank(idx_t w, idx_t* u, idx_t* v) {
     idx_t uu = (idx_t)((sqrt(8.0 * (double)w + 1.0) - 1.0) * 0.5);

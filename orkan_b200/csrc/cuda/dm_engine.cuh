@@ -179,7 +179,7 @@ ORKAN_HD void dm_setup(const Map& map, const DmGeom& g, idx_t w, DmPos* pd, unsi
     const unsigned npos = 1u << (2 * h);
     if (tid >= npos) return;
     idx_t u, v;
-    tri_unrank(w, &u, &v);
+    tri_unrank_f(w, &u, &v);
     const bool diag_item = (u == v);
     const idx_t rb = insert0_sorted(u, g.hb, h), cb = insert0_sorted(v, g.hb, h);
     const unsigned long long fm = g.fixrows;
@@ -225,13 +225,19 @@ ORKAN_HD void dm_setup(const Map& map, const DmGeom& g, idx_t w, DmPos* pd, unsi
         // the lower half, so none of their rows may be skipped
         const bool no_skip = Map::kMirrors && q.cls == kSubDiag;
         q.allvar = (fm && !no_skip && ((fm >> q.fvar) & smask) == smask) ? 1 : 0;
+        // bytes the position's lines bring in: whole S x S sub-tile, or the lower half of a
+        // diagonal one, less the lines skipped because every element in them is fixed
         unsigned bytes = 0;
         if (q.cls != kSubSkip) {
-            for (unsigned line = 0; line < S; ++line) {
-                if (dm_line_skipped(fm, q, line)) continue;
-                unsigned p0, p1;
-                dm_line_range<Map>(q, line, S, &p0, &p1);
-                bytes += (p1 - p0) * 16u;
+            const unsigned full = q.cls == kSubDiag ? S * (S + 1) / 2 : S * S;
+            bytes = full * 16u;
+            if (q.allvar) {
+                const unsigned long long skip = (fm >> q.fconst) & smask;
+                if (q.cls != kSubDiag) {
+                    bytes -= (unsigned)popc64(skip) * S * 16u;
+                } else {                                   // packed diagonal: line j holds S - j
+                    for (unsigned long long m = skip; m; m &= m - 1) bytes -= (S - ctz64(m)) * 16u;
+                }
             }
         }
         q.bytes = bytes;
@@ -515,10 +521,9 @@ inline void dm_orient(OpSuper1& op, bool transposed) {
     for (unsigned i = 0; i < 16; ++i) op.s[i] = t[i];
 }
 
-// Shared memory of one block of the pipelined engine: two mbarriers, then two stages of
-// (descriptors, staged block).
+// Shared memory of one engine block: the mbarrier, the descriptors, the staged block.
 ORKAN_HD size_t dm_stage_bytes(const DmGeom& g) { return kDmPosBytes + (size_t)g.V() * g.P() * 16; }
-ORKAN_HD size_t dm_pipe_smem_bytes(const DmGeom& g) { return 16 + 2 * dm_stage_bytes(g); }
+ORKAN_HD size_t dm_block_smem_bytes(const DmGeom& g) { return 16 + dm_stage_bytes(g); }
 
 // One work item, phase by phase (the CPU emulator runs each phase for all threads before
 // the next; the kernel below overlaps items with a two-stage pipeline).
@@ -538,8 +543,8 @@ ORKAN_HD void dm_engine_item_phase(int phase, const Mem& mem, const Map& map, co
 }
 constexpr int kDmPhases = 7;
 
-constexpr unsigned kDmBlock = 512;          // threads of the pipelined engine block
-constexpr unsigned kDmIssueThreads = 64;    // threads that issue the bulk copies
+constexpr unsigned kDmBlock = 256;          // threads of an engine block
+constexpr unsigned kDmIssueThreads = 32;    // threads (one warp) that issue the bulk copies
 
 #ifdef __CUDACC__
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -589,90 +594,69 @@ __device__ __forceinline__ bool dm_wait_stage(unsigned long long* bar, unsigned 
     return false;
 }
 
-// Persistent, double-buffered engine: block b handles items b, b + G, b + 2G, ...; the bulk
-// copies of the next item are in flight while the current one is fixed up, computed and
-// stored.  The staged block is read back to global memory with bulk stores.
+// Persistent engine: block b handles items b, b + G, b + 2G, ...  One item at a time per
+// block; with up to three blocks resident per SM (71 KB of shared memory each) the bulk
+// copies of one block's item overlap the compute and stores of the others.
 template <class Map, class Op>
 __global__ void __launch_bounds__(kDmBlock) k_dm_engine(DevMemBulk mem, Map map, DmGeom g, Op op) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem_raw);
-    const size_t stage = dm_stage_bytes(g);
-    DmPos* pd[2] = {reinterpret_cast<DmPos*>(smem_raw + 16), reinterpret_cast<DmPos*>(smem_raw + 16 + stage)};
-    double2* vb[2] = {reinterpret_cast<double2*>(smem_raw + 16 + kDmPosBytes),
-                      reinterpret_cast<double2*>(smem_raw + 16 + stage + kDmPosBytes)};
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw);
+    DmPos* pd = reinterpret_cast<DmPos*>(smem_raw + 16);
+    double2* vb = reinterpret_cast<double2*>(smem_raw + 16 + kDmPosBytes);
     const unsigned tid = threadIdx.x, nthr = blockDim.x;
     const unsigned npos = 1u << (2 * g.h);
-    idx_t w = blockIdx.x;
-    if (w >= g.items) return;
+    if (blockIdx.x >= g.items) return;
     if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        mbar_init(bar, 1);
         fence_mbar_init();
     }
-    dm_setup(map, g, w, pd[0], tid, nthr);
-    __syncthreads();
-    unsigned parity[2] = {0u, 0u};
-    if (tid == 0) {
-        unsigned bytes = 0;
-        for (unsigned t = 0; t < npos; ++t) bytes += pd[0][t].bytes;
-        mbar_arrive_expect(&bars[0], bytes);
-    }
-    __syncthreads();
-    if (tid < kDmIssueThreads) dm_bulk_loads(mem, map, g, pd[0], vb[0], &bars[0], tid, kDmIssueThreads);
+    unsigned parity = 0;
     bool ok = true;
-    for (unsigned it = 0;; ++it) {
-        const unsigned cur = it & 1u, nxt = cur ^ 1u;
-        const idx_t wn = w + gridDim.x;
-        const bool more = wn < g.items;
-        if (more) dm_setup(map, g, wn, pd[nxt], tid, nthr);
-        __syncthreads();                                    // pd[nxt] ready; vb[nxt] no longer read
-        if (more) {
+    for (idx_t w = blockIdx.x; w < g.items; w += gridDim.x) {
+        dm_setup(map, g, w, pd, tid, nthr);
+        __syncthreads();                                   // descriptors ready (and barrier initialised)
+        if (tid < 32) {                                     // warp 0 arms the barrier and issues the loads
             if (tid == 0) {
                 unsigned bytes = 0;
-                for (unsigned t = 0; t < npos; ++t) bytes += pd[nxt][t].bytes;
-                mbar_arrive_expect(&bars[nxt], bytes);
+                for (unsigned t = 0; t < npos; ++t) bytes += pd[t].bytes;
+                mbar_arrive_expect(bar, bytes);
             }
-            __syncthreads();
-            if (tid < kDmIssueThreads) {
-                fence_proxy_async();
-                dm_bulk_loads(mem, map, g, pd[nxt], vb[nxt], &bars[nxt], tid, kDmIssueThreads);
-            }
+            __syncwarp();
+            fence_proxy_async();
+            dm_bulk_loads(mem, map, g, pd, vb, bar, tid, 32u);
         }
-        ok = __syncthreads_and(dm_wait_stage(&bars[cur], parity[cur]) ? 1 : 0) != 0;
-        parity[cur] ^= 1u;
+        const unsigned long long fix0 = dm_pass_mask<Map>(pd, npos, 0);
+        const unsigned long long fix1 = dm_pass_mask<Map>(pd, npos, 1);
+        const unsigned long long mirr = dm_pass_mask<Map>(pd, npos, 2);
+        ok = __syncthreads_and(dm_wait_stage(bar, parity) ? 1 : 0) != 0;
+        parity ^= 1u;
         if (!ok) break;
-        const unsigned long long fix0 = dm_pass_mask<Map>(pd[cur], npos, 0);
-        const unsigned long long fix1 = dm_pass_mask<Map>(pd[cur], npos, 1);
-        const unsigned long long mirr = dm_pass_mask<Map>(pd[cur], npos, 2);
         if (fix0) {
-            dm_fixups<Map>(g, pd[cur], vb[cur], 0, fix0, tid, nthr);
+            dm_fixups<Map>(g, pd, vb, 0, fix0, tid, nthr);
             __syncthreads();
         }
-        op(g, vb[cur], tid, nthr);
+        op(g, vb, tid, nthr);
         __syncthreads();
         if (fix1) {
-            dm_fixups<Map>(g, pd[cur], vb[cur], 1, fix1, tid, nthr);
+            dm_fixups<Map>(g, pd, vb, 1, fix1, tid, nthr);
             __syncthreads();
         }
         fence_proxy_async();
         __syncthreads();
-        if (tid < kDmIssueThreads) {
-            dm_bulk_stores(mem, map, g, pd[cur], vb[cur], tid, kDmIssueThreads);
+        if (tid < 32) {
+            dm_bulk_stores(mem, map, g, pd, vb, tid, 32u);
             bulk_commit();
         }
-        if (mirr) dm_mirror_stores(mem, map, g, pd[cur], vb[cur], mirr, tid, nthr);
-        if (tid < kDmIssueThreads) bulk_wait_read();          // staged block free again
-        if (!more) break;
-        w = wn;
-        __syncthreads();       // every thread is done with stage cur before the next setup refills it
+        if (mirr) dm_mirror_stores(mem, map, g, pd, vb, mirr, tid, nthr);
+        if (tid < 32) bulk_wait_read();                     // the staged block may be refilled
+        __syncthreads();
     }
     if (!ok) {
-        // give the copies still in flight for the other stage a bounded chance to land
-        for (unsigned s = 0; s < 2; ++s)
-            for (unsigned long long i = 0; i < kDmWaitLimit && !mbar_try_wait(&bars[s], parity[s]); ++i) {
-            }
+        // give copies still in flight a bounded chance to land before the block exits
+        for (unsigned long long i = 0; i < kDmWaitLimit && !mbar_try_wait(bar, parity); ++i) {
+        }
     }
-    if (tid < kDmIssueThreads) bulk_wait_all();
+    if (tid < 32) bulk_wait_all();
 }
 #endif
 

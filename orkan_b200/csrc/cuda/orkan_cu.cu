@@ -66,7 +66,7 @@ unsigned engine_grid(Kern kern, size_t smem, idx_t items) {
 template <class Op>
 int launch_engine_map(int layout, unsigned log_tile, void* rho, unsigned n, const DmGeom& g, Op op,
                       cudaStream_t st) {
-    const size_t smem = dm_pipe_smem_bytes(g);
+    const size_t smem = dm_block_smem_bytes(g);
     dm_orient(op, layout == 1);               // the packed layout stages rho^T
     DevMemBulk mem{static_cast<double2*>(rho)};
     if (layout == 1) {
