@@ -55,9 +55,12 @@ struct DmGeom {
     ORKAN_HD unsigned P() const { return V() + 1; }    // smem row pitch (padded)
 };
 
-// Choose the sub-tile side: the largest S (<= smax) with V^2 <= kDmMaxElems.
+// Choose the sub-tile side: the largest S (<= 2^ls_max) whose block side V = S * 2^h stays
+// within the cap: max_v_low when at most one gate qubit lies above the sub-tile, 64
+// otherwise (keeping bulk-copy lines long when the block holds many sub-tiles).
 // qubits[j] is gate qubit j, qubits[0] the most significant bit of the local index.
-inline bool dm_geometry(unsigned n, unsigned k, const unsigned* qubits, unsigned ls_max, DmGeom* g) {
+inline bool dm_geometry(unsigned n, unsigned k, const unsigned* qubits, unsigned ls_max, DmGeom* g,
+                        unsigned max_v_low = kDmMaxV) {
     if (k < 1 || k > 3 || n < k) return false;
     for (unsigned j = 0; j < k; ++j) {
         if (qubits[j] >= n) return false;
@@ -67,7 +70,8 @@ inline bool dm_geometry(unsigned n, unsigned k, const unsigned* qubits, unsigned
     for (;; --ls) {
         unsigned h = 0;
         for (unsigned j = 0; j < k; ++j) h += (qubits[j] >= ls);
-        if ((1ull << (2 * (ls + h))) <= kDmMaxElems || ls == 0) {
+        const unsigned long long cap = h <= 1 ? (unsigned long long)max_v_low * max_v_low : kDmMaxElems;
+        if ((1ull << (2 * (ls + h))) <= cap || ls == 0) {
             g->d = idx_t(1) << n;
             g->n = n;
             g->ls = ls;

@@ -11,6 +11,7 @@
 #include "../../../include/orkan_cu.h"
 
 #include <atomic>
+#include <stdlib.h>
 #include <mutex>
 
 using namespace orkan;
@@ -79,6 +80,21 @@ int launch_engine_map(int layout, unsigned log_tile, void* rho, unsigned n, cons
         kern<<<grid, kDmBlock, smem, st>>>(mem, TiledMap{idx_t(1) << n, log_tile}, g, op);
     }
     return finish_launch();
+}
+
+// Largest engine block side when at most one gate qubit lies above the sub-tile (a power of
+// two in [8, 64]).  Tuning knob: environment variable ORKAN_DM_MAX_V, read once.
+unsigned dm_max_v_low() {
+    static unsigned v = 0;
+    if (!v) {
+        unsigned x = 32;
+        if (const char* e = getenv("ORKAN_DM_MAX_V")) {
+            const unsigned y = (unsigned)atoi(e);
+            if (y == 8 || y == 16 || y == 32 || y == 64) x = y;
+        }
+        v = x;
+    }
+    return v;
 }
 
 inline bool layout_ok(int layout, unsigned log_tile) {
@@ -191,7 +207,7 @@ int orkan_cu_dm_unitary(int layout, unsigned log_tile, void* rho, unsigned n, un
     if (!rho || !qubits || !u || !layout_ok(layout, log_tile) || (k != 1 && k != 2) || n > 40)
         return (int)cudaErrorInvalidValue;
     DmGeom g;
-    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g)) return (int)cudaErrorInvalidValue;
+    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g, dm_max_v_low())) return (int)cudaErrorInvalidValue;
     if (k == 1) {
         OpMix1 op;
         for (unsigned i = 0; i < 4; ++i) op.u[i] = ld_c(u, i);
@@ -215,7 +231,7 @@ int orkan_cu_dm_monomial(int layout, unsigned log_tile, void* rho, unsigned n, u
         op.phase[y] = ld_c(phase, y);
     }
     DmGeom g;
-    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g)) return (int)cudaErrorInvalidValue;
+    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g, dm_max_v_low())) return (int)cudaErrorInvalidValue;
     g.fixmask = monomial_fixmask(op, m);
     g.fixrows = dm_fixed_rows(g);
     return launch_engine_map(layout, log_tile, rho, n, g, op, as_stream(stream));
@@ -247,7 +263,7 @@ int orkan_cu_dm_superop1(int layout, unsigned log_tile, void* rho, unsigned n, u
     for (unsigned i = 0; i < 16; ++i) op.s[i] = ld_c(sop, i);
     DmGeom g;
     const unsigned q[1] = {target};
-    if (!dm_geometry(n, 1, q, ls_max_for(layout, log_tile), &g)) return (int)cudaErrorInvalidValue;
+    if (!dm_geometry(n, 1, q, ls_max_for(layout, log_tile), &g, dm_max_v_low())) return (int)cudaErrorInvalidValue;
     return launch_engine_map(layout, log_tile, rho, n, g, op, as_stream(stream));
 }
 

@@ -14,6 +14,7 @@
 #include "../../orkan_b200/csrc/cuda/pure.cuh"
 
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 #include <vector>
 
@@ -115,6 +116,16 @@ int engine_dispatch(int layout, unsigned log_tile, double* rho, idx_t len, unsig
 
 unsigned ls_max_for(int layout, unsigned log_tile) { return layout == 2 ? log_tile : 6u; }
 
+// block-side cap of the engine (the GPU default 32, or ORKAN_DM_MAX_V)
+unsigned emu_max_v() {
+    unsigned x = 32;
+    if (const char* e = getenv("ORKAN_DM_MAX_V")) {
+        const unsigned y = (unsigned)atoi(e);
+        if (y == 8 || y == 16 || y == 32 || y == 64) x = y;
+    }
+    return x;
+}
+
 template <class Factor>
 void run_phase(int layout, unsigned log_tile, const EmuMem& mem, unsigned n, const Factor& fac) {
     const PhaseGeom g = phase_geometry(n, layout == 2 ? log_tile : 5u);
@@ -138,7 +149,7 @@ extern "C" {
 int emu_dm_unitary(int layout, unsigned log_tile, double* rho, uint64_t len, unsigned n, unsigned k,
                    const unsigned* qubits, const double* u, uint32_t* reads, uint32_t* writes, uint64_t* oob) {
     DmGeom g;
-    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g)) return -1;
+    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g, emu_max_v())) return -1;
     if (k == 1) {
         OpMix1 op;
         for (unsigned i = 0; i < 4; ++i) op.u[i] = ldc(u, i);
@@ -156,7 +167,7 @@ int emu_dm_monomial(int layout, unsigned log_tile, double* rho, uint64_t len, un
     for (unsigned y = 0; y < 8; ++y) { op.src[y] = y; op.phase[y] = c2(1.0, 0.0); }
     for (unsigned y = 0; y < (1u << k); ++y) { op.src[y] = src[y]; op.phase[y] = ldc(phase, y); }
     DmGeom g;
-    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g)) return -1;
+    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g, emu_max_v())) return -1;
     g.fixmask = monomial_fixmask(op, 1u << k);
     g.fixrows = dm_fixed_rows(g);
     return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
@@ -168,7 +179,7 @@ int emu_dm_superop1(int layout, unsigned log_tile, double* rho, uint64_t len, un
     for (unsigned i = 0; i < 16; ++i) op.s[i] = ldc(sop, i);
     DmGeom g;
     const unsigned q[1] = {target};
-    if (!dm_geometry(n, 1, q, ls_max_for(layout, log_tile), &g)) return -1;
+    if (!dm_geometry(n, 1, q, ls_max_for(layout, log_tile), &g, emu_max_v())) return -1;
     return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
 }
 
