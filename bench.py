@@ -397,6 +397,17 @@ def run_gpu(args):
                 "algorithmic_bytes_per_launch": avg_bytes, "avg_launch_ms": avg_ms, "launches": launches_dom}
     classes = {c: {"launches": per_class_n[c], "ms": per_class_ms[c], "share": per_class_ms[c] / sum(per_class_ms.values()),
                    "GB/s": per_class_bytes[c] / (per_class_ms[c] * 1e-3) / 1e9} for c in sorted(per_class_ms)}
+    by_gate = {}
+    for k in range(args.steps):
+        prev = start if k == 0 else ev[k - 1][-1]
+        for i, e in enumerate(plan):
+            dt = prev.elapsed_time(ev[k][i])
+            prev = ev[k][i]
+            key = f"{e[0]}:{e[2]}"
+            t = by_gate.setdefault(key, [0.0, 0])
+            t[0] += dt
+            t[1] += e[5]
+    gates = {key: {"ms": v[0], "GB/s": v[1] / (v[0] * 1e-3) / 1e9} for key, v in sorted(by_gate.items())}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -418,7 +429,7 @@ def run_gpu(args):
                            "l2": "inputs larger than L2 (16 GiB and 2.15 GB states vs 126 MB L2); no flush",
                            "parallelism": f"replicas x{world}"},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-                "gpu_launches": launches, "kernel_classes": classes}
+                "gpu_launches": launches, "kernel_classes": classes, "by_gate": gates}
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

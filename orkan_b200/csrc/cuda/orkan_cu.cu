@@ -87,7 +87,7 @@ int launch_engine_map(int layout, unsigned log_tile, void* rho, unsigned n, cons
 unsigned dm_max_v_low() {
     static unsigned v = 0;
     if (!v) {
-        unsigned x = 32;
+        unsigned x = 64;
         if (const char* e = getenv("ORKAN_DM_MAX_V")) {
             const unsigned y = (unsigned)atoi(e);
             if (y == 8 || y == 16 || y == 32 || y == 64) x = y;

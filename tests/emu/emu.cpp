@@ -116,9 +116,9 @@ int engine_dispatch(int layout, unsigned log_tile, double* rho, idx_t len, unsig
 
 unsigned ls_max_for(int layout, unsigned log_tile) { return layout == 2 ? log_tile : 6u; }
 
-// block-side cap of the engine (the GPU default 32, or ORKAN_DM_MAX_V)
+// block-side cap of the engine (the GPU default 64, or ORKAN_DM_MAX_V)
 unsigned emu_max_v() {
-    unsigned x = 32;
+    unsigned x = 64;
     if (const char* e = getenv("ORKAN_DM_MAX_V")) {
         const unsigned y = (unsigned)atoi(e);
         if (y == 8 || y == 16 || y == 32 || y == 64) x = y;
