@@ -386,3 +386,39 @@ def plus_state(kind: str, n: int) -> np.ndarray:
     if kind == "pure":
         return np.full(d, 1.0 / np.sqrt(float(d)), dtype=np.complex128)
     return np.full((d, d), 1.0 / d, dtype=np.complex128)
+
+
+# ----------------------------------------------------------------------------------------
+# QAOA-style circuits as compositions of reference calls (the batched entry point's checker)
+# ----------------------------------------------------------------------------------------
+def maxcut_cost(n: int, edges, weights=None) -> np.ndarray:
+    """cost[x] = sum_e w_e [bit u_e of x != bit v_e of x], summed in edge order."""
+    x = np.arange(1 << n, dtype=np.int64)
+    cost = np.zeros(1 << n, dtype=np.float64)
+    for e, (u, v) in enumerate(edges):
+        w = 1.0 if weights is None else float(weights[e])
+        cost += w * (((x >> u) ^ (x >> v)) & 1)
+    return cost
+
+
+def qaoa_state(n: int, cost: np.ndarray, gammas, betas, low_qubits: int | None = None,
+               layers: int | None = None, last_half: str | None = None) -> np.ndarray:
+    """state_plus (src/state/state_pure.c:30-43), then per layer k: exp_diag(cost, gamma_k)
+    (src/circ/circ_pure.c:21-33) and rx(q, 2 beta_k) on every qubit (src/gate/gate_pure.c:
+    230-234).  `layers` stops after that many layers; `last_half` = "low" / "high" applies
+    only the rx on qubits < low_qubits / >= low_qubits in the last layer."""
+    psi = plus_state("pure", n)
+    nl = len(gammas) if layers is None else layers
+    for k in range(nl):
+        psi = exp_diag("pure", psi, cost, float(gammas[k]))
+        qs = range(n)
+        if k == nl - 1 and last_half is not None:
+            qs = range(low_qubits) if last_half == "low" else range(low_qubits, n)
+        for q in qs:
+            psi = apply_pure(psi, "rx", [q], 2.0 * float(betas[k]))
+    return psi
+
+
+def qaoa_mean(n: int, cost: np.ndarray, gammas, betas) -> float:
+    """mean(cost) of the QAOA state (src/meas/meas_pure.c:20-30)."""
+    return mean("pure", qaoa_state(n, cost, gammas, betas), cost)

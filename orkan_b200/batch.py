@@ -1,0 +1,138 @@
+"""Binding of the batched QAOA entry points (include/orkan_batch.h) in liborkan_b200.so.
+
+    b = QaoaBatch(ork, n_list, edges_list, weights_list, p)
+    means = b.run(gammas, betas)          # [count][p] angles in instance order -> [count] means
+    b.tune(gammas, betas, cache_path)     # autotune chunk and block size per qubit count
+    b.close()
+
+Every call goes to the compiled library; there is no Python fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import OrkanError
+
+
+def _declare(lib):
+    if getattr(lib, "_qaoa_declared", False):
+        return
+    P = C.c_void_p
+    lib.orkan_qaoa_create.argtypes = [C.POINTER(P), C.c_uint, P, P, P, P, C.c_uint, C.c_ulonglong, C.c_uint]
+    lib.orkan_qaoa_run.argtypes = [P, P, P, P, P]
+    lib.orkan_qaoa_tune.argtypes = [P, P, P, C.c_char_p]
+    lib.orkan_qaoa_config.argtypes = [P, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]
+    lib.orkan_qaoa_cost_vector.argtypes = [P, C.c_uint, P]
+    lib.orkan_qaoa_stats.argtypes = [P, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]
+    lib.orkan_qaoa_destroy.argtypes = [P]
+    lib.orkan_qaoa_destroy.restype = None
+    for f in ("create", "run", "tune", "config", "cost_vector", "stats"):
+        getattr(lib, "orkan_qaoa_" + f).restype = C.c_int
+    lib._qaoa_declared = True
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise OrkanError(f"orkan_qaoa_{what} failed with CUDA error {rc}")
+
+
+class QaoaBatch:
+    """count instances of MaxCut-cost QAOA circuits with a shared depth p."""
+
+    def __init__(self, ork, n_qubits, edges, weights=None, p: int = 1, mem_budget: int = 0,
+                 f64_costs: bool = False):
+        self.lib = ork.lib
+        _declare(self.lib)
+        self.n = np.ascontiguousarray(n_qubits, dtype=np.uint32)
+        self.count, self.p = len(self.n), int(p)
+        off = np.zeros(self.count + 1, dtype=np.uint32)
+        flat = []
+        wflat = []
+        for i, es in enumerate(edges):
+            off[i + 1] = off[i] + len(es)
+            flat.extend(int(v) for e in es for v in e)
+            if weights is not None:
+                wflat.extend(float(x) for x in weights[i])
+        self._off = off
+        self._edges = np.ascontiguousarray(flat if flat else [0], dtype=np.uint32)
+        self._w = np.ascontiguousarray(wflat, dtype=np.float64) if weights is not None else None
+        h = C.c_void_p()
+        rc = self.lib.orkan_qaoa_create(C.byref(h), self.count, self.n.ctypes.data, off.ctypes.data,
+                                        self._edges.ctypes.data,
+                                        None if self._w is None else self._w.ctypes.data, self.p,
+                                        int(mem_budget), 1 if f64_costs else 0)
+        _check(rc, "create")
+        self.h = h
+
+    def _angles(self, gammas, betas):
+        g = np.ascontiguousarray(gammas, dtype=np.float64).reshape(self.count, self.p)
+        b = np.ascontiguousarray(betas, dtype=np.float64).reshape(self.count, self.p)
+        return g, b
+
+    def run(self, gammas, betas, stream: int | None = None) -> np.ndarray:
+        g, b = self._angles(gammas, betas)
+        out = np.empty(self.count, dtype=np.float64)
+        _check(self.lib.orkan_qaoa_run(self.h, g.ctypes.data, b.ctypes.data, out.ctypes.data, stream), "run")
+        return out
+
+    def tune(self, gammas, betas, cache_path: str | None = None) -> None:
+        g, b = self._angles(gammas, betas)
+        path = None if cache_path is None else cache_path.encode()
+        _check(self.lib.orkan_qaoa_tune(self.h, g.ctypes.data, b.ctypes.data, path), "tune")
+
+    def config(self, n: int) -> tuple[int, int]:
+        lc, t = C.c_uint(), C.c_uint()
+        _check(self.lib.orkan_qaoa_config(self.h, n, C.byref(lc), C.byref(t)), "config")
+        return lc.value, t.value
+
+    def cost_vector(self, i: int) -> np.ndarray:
+        out = np.empty(1 << int(self.n[i]), dtype=np.float64)
+        _check(self.lib.orkan_qaoa_cost_vector(self.h, i, out.ctypes.data), "cost_vector")
+        return out
+
+    def stats(self) -> tuple[int, int]:
+        w, l = C.c_uint(), C.c_uint()
+        _check(self.lib.orkan_qaoa_stats(self.h, C.byref(w), C.byref(l)), "stats")
+        return w.value, l.value
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.orkan_qaoa_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def random_regular_graph(n: int, d: int, rng) -> list[tuple[int, int]]:
+    """A uniformly drawn simple d-regular graph on n vertices (configuration model with
+    rejection of loops and multi-edges).  When n * d is odd no such graph exists; then one
+    random vertex gets degree d - 1 and all others degree d."""
+    if d >= n:
+        raise ValueError("degree must be below the vertex count")
+    deg = np.full(n, d)
+    if (n * d) % 2:
+        deg[rng.integers(n)] -= 1
+    while True:
+        stubs = rng.permutation(np.repeat(np.arange(n), deg))
+        pairs = stubs.reshape(-1, 2)
+        if np.any(pairs[:, 0] == pairs[:, 1]):
+            continue
+        key = {tuple(sorted(map(int, e))) for e in pairs}
+        if len(key) == len(pairs):
+            return [tuple(int(v) for v in e) for e in pairs]
+
+
+def erdos_renyi_graph(n: int, prob: float, rng) -> list[tuple[int, int]]:
+    return [(u, v) for u in range(n) for v in range(u + 1, n) if rng.random() < prob]

@@ -213,15 +213,15 @@ __global__ void __launch_bounds__(kPureThreads) k_pure2q(DevMem mem, idx_t nquad
     pure2q_thread<OP>(mem, nquads, qc, qt, (idx_t)blockIdx.x * blockDim.x + threadIdx.x,
                       (idx_t)gridDim.x * blockDim.x);
 }
-__global__ void __launch_bounds__(kPureThreads) k_pure_ccx(DevMem mem, idx_t noct, unsigned c1, unsigned c2q, unsigned t) {
+static __global__ void __launch_bounds__(kPureThreads) k_pure_ccx(DevMem mem, idx_t noct, unsigned c1, unsigned c2q, unsigned t) {
     pure_ccx_thread(mem, noct, c1, c2q, t, (idx_t)blockIdx.x * blockDim.x + threadIdx.x,
                     (idx_t)gridDim.x * blockDim.x);
 }
-__global__ void __launch_bounds__(kPureThreads) k_pure_exp_diag(DevMem mem, DevMemR diag, idx_t dim, double t) {
+static __global__ void __launch_bounds__(kPureThreads) k_pure_exp_diag(DevMem mem, DevMemR diag, idx_t dim, double t) {
     pure_exp_diag_thread(mem, diag, dim, t, (idx_t)blockIdx.x * blockDim.x + threadIdx.x,
                          (idx_t)gridDim.x * blockDim.x);
 }
-__global__ void __launch_bounds__(kPureThreads) k_fill(DevMem mem, idx_t len, double2 val, unsigned clt, idx_t cdim) {
+static __global__ void __launch_bounds__(kPureThreads) k_fill(DevMem mem, idx_t len, double2 val, unsigned clt, idx_t cdim) {
     fill_thread(mem, len, val, clt, cdim, (idx_t)blockIdx.x * blockDim.x + threadIdx.x,
                 (idx_t)gridDim.x * blockDim.x);
 }

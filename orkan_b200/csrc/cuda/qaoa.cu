@@ -1,0 +1,642 @@
+// qaoa.cu - the batched QAOA entry points of include/orkan_batch.h: the batch context,
+// resident cost vectors (one per distinct graph), waves of state vectors, the fused pass
+// kernels, one CUDA graph per batch and the autotuner of the launch configuration.
+#include "qaoa.cuh"
+
+#include "../../../include/orkan_batch.h"
+
+#include <stdint.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+using namespace orkan;
+
+namespace {
+
+template <class CostT>
+struct DevCost {
+    const CostT* p;
+    __device__ __forceinline__ CostT ld(idx_t i) const { return __ldg(p + i); }
+};
+
+// cost[x] = sum_e w_e [bit u_e of x != bit v_e of x], edges in the given order.
+template <class CostT>
+__global__ void k_qaoa_cost(CostT* cost, unsigned n, const unsigned char* edges, const double* w, unsigned ne) {
+    const idx_t dim = idx_t(1) << n;
+    for (idx_t x = (idx_t)blockIdx.x * blockDim.x + threadIdx.x; x < dim; x += (idx_t)gridDim.x * blockDim.x) {
+        double c = 0.0;
+        for (unsigned e = 0; e < ne; ++e)
+            if (((x >> edges[2 * e]) ^ (x >> edges[2 * e + 1])) & 1u) c += w[e];
+        cost[x] = (CostT)c;
+    }
+}
+
+// table[(pos p + k) tstride + c] = (cos, sin)(c * gamma[pos p + k]) for c <= cmax of pos
+__global__ void k_qaoa_tables(const unsigned* cmax, const double* gamma, unsigned count, unsigned p,
+                              unsigned tstride, double2* table) {
+    const unsigned pos = blockIdx.x;
+    if (pos >= count || cmax[pos] >= kQaoaMaxTable) return;
+    const unsigned m = cmax[pos] + 1;
+    for (unsigned t = threadIdx.x; t < p * m; t += blockDim.x) {
+        const unsigned k = t / m, c = t % m;
+        double sn, cs;
+        sincos((double)c * gamma[(idx_t)pos * p + k], &sn, &cs);
+        table[((idx_t)pos * p + k) * tstride + c] = c2(cs, sn);
+    }
+}
+
+template <unsigned NT, class CostT>
+__global__ void __launch_bounds__(NT) k_qaoa_pass(QaoaPass P, QaoaTables T) {
+    extern __shared__ double2 smem_q[];
+    QaoaSmem<CostT> S;
+    S.vb = smem_q;
+    S.red = reinterpret_cast<double*>(smem_q + (1u << P.C));
+    S.cb = reinterpret_cast<CostT*>(S.red + NT + 32);
+    for (idx_t w = blockIdx.x; w < P.items; w += gridDim.x) {
+        const QaoaInst I = P.inst[qaoa_find(P.inst, P.ninst, w)];
+        const QaoaPlan pl = qaoa_plan(I.n, P.C, P.kind, P.p, P.pass);
+        const unsigned nst = qaoa_stages(pl);
+        const DevMem psi{I.psi};
+        const DevCost<CostT> cost{static_cast<const CostT*>(I.cost)};
+        for (unsigned st = 0; st < nst; ++st) {
+            qaoa_stage<CostT>(P, T, I, pl, psi, cost, w - I.item0, st, S, threadIdx.x, NT);
+            __syncthreads();
+        }
+    }
+}
+
+// out[pos] = sum of the instance's chunk partials, in chunk order
+__global__ void k_qaoa_fold(const QaoaInst* inst, unsigned ninst, const double* partial, idx_t items, double* out) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ninst) return;
+    const idx_t a = inst[i].item0, b = (i + 1 < ninst) ? inst[i + 1].item0 : items;
+    double s = 0.0;
+    for (idx_t w = a; w < b; ++w) s += partial[w];
+    out[inst[i].pos] = s;
+}
+
+int sm_count() {
+    int dev = 0, v = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+}
+
+template <unsigned NT, class CostT>
+int pass_grid(size_t smem, idx_t items, unsigned* grid) {
+    static bool attr = false;
+    if (!attr) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(k_qaoa_pass<NT, CostT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        if (e != cudaSuccess) return (int)e;
+        attr = true;
+    }
+    int per = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_qaoa_pass<NT, CostT>, NT, smem);
+    if (e != cudaSuccess) return (int)e;
+    if (per < 1) return (int)cudaErrorInvalidConfiguration;
+    const idx_t cap = (idx_t)sm_count() * per;
+    *grid = (unsigned)(items < cap ? items : cap);
+    return 0;
+}
+
+// Blocks of a pass launch: every item gets a block, up to the resident blocks of all SMs.
+// (Called before any graph capture: it sets the kernel's shared-memory attribute.)
+template <class CostT>
+int pass_grid_t(unsigned nt, unsigned C, idx_t items, unsigned* grid) {
+    const size_t smem = qaoa_smem_bytes<CostT>(C, nt);
+    return nt == 256 ? pass_grid<256, CostT>(smem, items, grid) : pass_grid<512, CostT>(smem, items, grid);
+}
+
+template <class CostT>
+int launch_pass_t(unsigned nt, unsigned grid, const QaoaPass& P, const QaoaTables& T, cudaStream_t st) {
+    const size_t smem = qaoa_smem_bytes<CostT>(P.C, nt);
+    if (nt == 256) k_qaoa_pass<256, CostT><<<grid, 256, smem, st>>>(P, T);
+    else k_qaoa_pass<512, CostT><<<grid, 512, smem, st>>>(P, T);
+    return (int)cudaGetLastError();
+}
+
+struct Graph {                     // one distinct cost function
+    unsigned n;
+    std::vector<unsigned char> edges;
+    std::vector<double> w;
+    unsigned cmax;                 // byte costs: integer maximum; else 0xffffffff
+    void* d_cost = nullptr;
+};
+
+struct Launch {
+    int what;                      // 0 pass, 1 fold
+    unsigned inst_off, ninst;      // slice of the plan's instance records
+    idx_t items;
+    unsigned pass, C, kind, nt;
+    unsigned grid;                 // blocks (pass launches)
+    bool bytes;                    // byte costs
+    size_t partial_off;
+};
+
+struct Plan {
+    std::vector<Launch> launches;
+    std::vector<QaoaInst> inst;    // psi holds an arena offset until the arena is known
+    size_t arena = 0, partial = 0;
+    unsigned waves = 0;
+};
+
+}  // namespace
+
+struct orkan_qaoa {
+    int device = 0;
+    unsigned count = 0, p = 0;
+    std::vector<unsigned> n;            // by instance
+    std::vector<unsigned> gid;          // graph of each instance
+    std::vector<Graph> graphs;
+    std::vector<unsigned> cmax;         // by instance (byte costs) or 0xffffffff
+    unsigned tstride = 1;
+    bool any_bytes = false;
+    unsigned long long budget = 0;
+    unsigned cfgC[27], cfgT[27];        // launch configuration by qubit count
+    // device buffers
+    unsigned* d_cmax = nullptr;
+    double* d_gamma = nullptr;          // [instance][p]
+    double2* d_rx = nullptr;
+    double2* d_table = nullptr;         // [instance][p][tstride]
+    double* d_out = nullptr;
+    double* d_partial = nullptr;
+    unsigned char* d_arena = nullptr;
+    size_t arena_bytes = 0, partial_cap = 0;
+    QaoaInst* d_inst = nullptr;
+    size_t inst_cap = 0;
+    // pinned host staging
+    double* h_gamma = nullptr;
+    double2* h_rx = nullptr;
+    double* h_out = nullptr;
+    Plan plan;
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+template <class T>
+int dalloc(T** p, size_t count) {
+    return (int)cudaMalloc(reinterpret_cast<void**>(p), (count ? count : 1) * sizeof(T));
+}
+
+unsigned default_C(unsigned n) { return n <= kQaoaMaxC ? n : kQaoaMaxC; }
+bool is_full(const orkan_qaoa* b, unsigned n) { return n <= b->cfgC[n]; }
+size_t state_bytes(const orkan_qaoa* b, unsigned n) { return is_full(b, n) ? 0 : (size_t(1) << n) * 16; }
+
+// Launch plan for the instances `sel` (qubit counts descending), in waves under the budget.
+Plan make_plan(const orkan_qaoa* b, const std::vector<unsigned>& sel) {
+    Plan pl;
+    size_t first = 0;
+    while (first < sel.size()) {
+        size_t bytes = 0, last = first;
+        while (last < sel.size() && (last == first || bytes + state_bytes(b, b->n[sel[last]]) <= b->budget))
+            bytes += state_bytes(b, b->n[sel[last++]]);
+        pl.arena = std::max(pl.arena, bytes);
+        ++pl.waves;
+        std::vector<size_t> off(last - first);              // state offsets of the wave
+        size_t o = 0;
+        for (size_t k = first; k < last; ++k) {
+            off[k - first] = o;
+            o += state_bytes(b, b->n[sel[k]]);
+        }
+        size_t partial = 0;
+        size_t g0 = first;                                  // one group per (qubit count, cost type)
+        while (g0 < last) {
+            const unsigned nq = b->n[sel[g0]];
+            for (int bytes_cost = 1; bytes_cost >= 0; --bytes_cost) {
+                std::vector<size_t> grp;
+                for (size_t k = g0; k < last && b->n[sel[k]] == nq; ++k)
+                    if ((b->cmax[sel[k]] < kQaoaMaxTable) == (bool)bytes_cost) grp.push_back(k);
+                if (grp.empty()) continue;
+                const bool full = is_full(b, nq);
+                const unsigned C = full ? nq : b->cfgC[nq];
+                const unsigned npass = full ? 1 : b->p + 1;
+                Launch meas{};
+                for (unsigned j = 0; j < npass; ++j) {
+                    Launch L{};
+                    L.what = 0;
+                    L.inst_off = (unsigned)pl.inst.size();
+                    L.ninst = (unsigned)grp.size();
+                    L.pass = full ? 0 : j;
+                    L.C = C;
+                    L.kind = full ? kQaoaFull : ((j % 2 == 0) ? kQaoaLow : kQaoaHigh);
+                    L.nt = b->cfgT[nq];
+                    L.bytes = bytes_cost;
+                    idx_t acc = 0;
+                    for (size_t k : grp) {
+                        QaoaInst r;
+                        r.psi = reinterpret_cast<double2*>(off[k - first]);
+                        r.cost = b->graphs[b->gid[sel[k]]].d_cost;
+                        r.item0 = acc;
+                        r.n = nq;
+                        r.pos = sel[k];
+                        acc += qaoa_items(nq, C, L.kind);
+                        pl.inst.push_back(r);
+                    }
+                    L.items = acc;
+                    if (j + 1 == npass) {
+                        L.partial_off = partial;
+                        partial += (size_t)acc;
+                        meas = L;
+                    }
+                    pl.launches.push_back(L);
+                }
+                meas.what = 1;
+                pl.launches.push_back(meas);
+            }
+            while (g0 < last && b->n[sel[g0]] == nq) ++g0;
+        }
+        pl.partial = std::max(pl.partial, partial);
+        first = last;
+    }
+    return pl;
+}
+
+// Device side of a plan: arena, partial sums and the instance records.
+int upload_plan(orkan_qaoa* b, Plan& pl) {
+    int rc;
+    if (pl.arena > b->arena_bytes) {
+        cudaFree(b->d_arena);
+        b->d_arena = nullptr;
+        b->arena_bytes = 0;
+        if ((rc = dalloc(&b->d_arena, pl.arena))) return rc;
+        b->arena_bytes = pl.arena;
+    }
+    if (pl.partial > b->partial_cap) {
+        cudaFree(b->d_partial);
+        b->d_partial = nullptr;
+        b->partial_cap = 0;
+        if ((rc = dalloc(&b->d_partial, pl.partial))) return rc;
+        b->partial_cap = pl.partial;
+    }
+    for (auto& L : pl.launches) {
+        if (L.what != 0) continue;
+        rc = L.bytes ? pass_grid_t<uint8_t>(L.nt, L.C, L.items, &L.grid) : pass_grid_t<double>(L.nt, L.C, L.items, &L.grid);
+        if (rc) return rc;
+    }
+    for (auto& r : pl.inst) r.psi = reinterpret_cast<double2*>(b->d_arena + reinterpret_cast<size_t>(r.psi));
+    if (pl.inst.size() > b->inst_cap) {
+        cudaFree(b->d_inst);
+        b->d_inst = nullptr;
+        b->inst_cap = 0;
+        if ((rc = dalloc(&b->d_inst, pl.inst.size()))) return rc;
+        b->inst_cap = pl.inst.size();
+    }
+    return (int)cudaMemcpy(b->d_inst, pl.inst.data(), pl.inst.size() * sizeof(QaoaInst), cudaMemcpyHostToDevice);
+}
+
+// The device work of a plan (no copies).
+int enqueue_kernels(const orkan_qaoa* b, const Plan& pl, cudaStream_t st) {
+    const QaoaTables T{b->d_table, b->d_rx, b->tstride};
+    for (const auto& L : pl.launches) {
+        const QaoaInst* inst = b->d_inst + L.inst_off;
+        int rc = 0;
+        if (L.what == 0) {
+            QaoaPass P;
+            P.inst = inst;
+            P.ninst = L.ninst;
+            P.items = L.items;
+            P.gamma = b->d_gamma;
+            P.partial = b->d_partial + L.partial_off;
+            P.p = b->p;
+            P.pass = L.pass;
+            P.C = L.C;
+            P.kind = L.kind;
+            rc = L.bytes ? launch_pass_t<uint8_t>(L.nt, L.grid, P, T, st) : launch_pass_t<double>(L.nt, L.grid, P, T, st);
+        } else {
+            k_qaoa_fold<<<(L.ninst + 127) / 128, 128, 0, st>>>(inst, L.ninst, b->d_partial + L.partial_off, L.items,
+                                                               b->d_out);
+            rc = (int)cudaGetLastError();
+        }
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+int enqueue_tables(const orkan_qaoa* b, cudaStream_t st) {
+    if (!b->any_bytes) return 0;
+    k_qaoa_tables<<<b->count, 128, 0, st>>>(b->d_cmax, b->d_gamma, b->count, b->p, b->tstride, b->d_table);
+    return (int)cudaGetLastError();
+}
+
+// One evaluation: angles in, tables, the plan's kernels, means out.
+int enqueue_run(const orkan_qaoa* b, const Plan& pl, cudaStream_t st) {
+    const size_t np = (size_t)b->count * b->p;
+    int rc;
+    if ((rc = (int)cudaMemcpyAsync(b->d_gamma, b->h_gamma, np * 8, cudaMemcpyHostToDevice, st))) return rc;
+    if ((rc = (int)cudaMemcpyAsync(b->d_rx, b->h_rx, np * 16, cudaMemcpyHostToDevice, st))) return rc;
+    if ((rc = enqueue_tables(b, st))) return rc;
+    if ((rc = enqueue_kernels(b, pl, st))) return rc;
+    return (int)cudaMemcpyAsync(b->h_out, b->d_out, (size_t)b->count * 8, cudaMemcpyDeviceToHost, st);
+}
+
+int rebuild(orkan_qaoa* b) {
+    std::vector<unsigned> sel(b->count);
+    for (unsigned i = 0; i < b->count; ++i) sel[i] = i;
+    std::stable_sort(sel.begin(), sel.end(), [&](unsigned a, unsigned c) { return b->n[a] > b->n[c]; });
+    Plan pl = make_plan(b, sel);
+    int rc = upload_plan(b, pl);
+    if (rc) return rc;
+    b->plan = pl;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    if ((rc = (int)cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal))) return rc;
+    const int erc = enqueue_run(b, b->plan, b->cap);
+    rc = (int)cudaStreamEndCapture(b->cap, &g);
+    if (erc || rc) {
+        if (g) cudaGraphDestroy(g);
+        return erc ? erc : rc;
+    }
+    rc = (int)cudaGraphInstantiate(&b->exec, g, 0);
+    cudaGraphDestroy(g);
+    return rc;
+}
+
+// Angles into the pinned staging buffers; rx coefficients with the host's libm, as the
+// per-call rx takes them (cos(theta / 2), sin(theta / 2) with theta = 2 beta).
+void stage_angles(orkan_qaoa* b, const double* gammas, const double* betas) {
+    const size_t np = (size_t)b->count * b->p;
+    for (size_t k = 0; k < np; ++k) {
+        const double theta = 2.0 * betas[k];
+        b->h_gamma[k] = gammas[k];
+        b->h_rx[k] = c2(cos(theta / 2.0), sin(theta / 2.0));
+    }
+}
+
+std::string cache_key(const orkan_qaoa* b, unsigned nq, bool bytes) {
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, b->device);
+    return std::string(prop.name) + "|n" + std::to_string(nq) + "|p" + std::to_string(b->p) + (bytes ? "|u8" : "|f64");
+}
+
+}  // namespace
+
+extern "C" {
+
+int orkan_qaoa_create(orkan_qaoa_t** out, unsigned count, const unsigned* n_qubits, const unsigned* edge_offsets,
+                      const unsigned* edges, const double* weights, unsigned p, unsigned long long mem_budget,
+                      unsigned flags) {
+    if (!out) return (int)cudaErrorInvalidValue;
+    *out = nullptr;
+    if (!count || !n_qubits || !edge_offsets || p == 0 || p > 64) return (int)cudaErrorInvalidValue;
+    for (unsigned i = 0; i < count; ++i) {
+        if (n_qubits[i] < 1 || n_qubits[i] > 26 || edge_offsets[i + 1] < edge_offsets[i])
+            return (int)cudaErrorInvalidValue;
+        for (unsigned e = edge_offsets[i]; e < edge_offsets[i + 1]; ++e)
+            if (!edges || edges[2 * e] >= n_qubits[i] || edges[2 * e + 1] >= n_qubits[i] ||
+                edges[2 * e] == edges[2 * e + 1])
+                return (int)cudaErrorInvalidValue;
+    }
+    orkan_qaoa* b = new orkan_qaoa();
+    cudaGetDevice(&b->device);
+    b->count = count;
+    b->p = p;
+    b->n.assign(n_qubits, n_qubits + count);
+    for (unsigned q = 0; q <= 26; ++q) {
+        b->cfgC[q] = default_C(q);
+        b->cfgT[q] = 512;
+    }
+    // distinct graphs (same qubit count, edges in the same order, same weights)
+    std::map<std::vector<unsigned char>, unsigned> seen;
+    b->gid.resize(count);
+    b->cmax.resize(count);
+    unsigned cm_all = 0;
+    int rc = 0;
+    for (unsigned i = 0; i < count; ++i) {
+        Graph g;
+        g.n = n_qubits[i];
+        double wsum = 0.0;
+        bool integral = true;
+        for (unsigned e = edge_offsets[i]; e < edge_offsets[i + 1]; ++e) {
+            g.edges.push_back((unsigned char)edges[2 * e]);
+            g.edges.push_back((unsigned char)edges[2 * e + 1]);
+            const double w = weights ? weights[e] : 1.0;
+            g.w.push_back(w);
+            if (!(w >= 0.0 && w == std::floor(w))) integral = false;
+            wsum += w;
+        }
+        g.cmax = (integral && wsum < kQaoaMaxTable && !(flags & ORKAN_QAOA_F64_COSTS)) ? (unsigned)wsum : 0xffffffffu;
+        std::vector<unsigned char> key(1, (unsigned char)g.n);
+        key.insert(key.end(), g.edges.begin(), g.edges.end());
+        const unsigned char* wb = reinterpret_cast<const unsigned char*>(g.w.data());
+        key.insert(key.end(), wb, wb + g.w.size() * 8);
+        auto it = seen.find(key);
+        unsigned id;
+        if (it == seen.end()) {
+            id = (unsigned)b->graphs.size();
+            seen.emplace(key, id);
+            b->graphs.push_back(g);
+        } else {
+            id = it->second;
+        }
+        b->gid[i] = id;
+        b->cmax[i] = b->graphs[id].cmax;
+        if (b->cmax[i] != 0xffffffffu) {
+            cm_all = std::max(cm_all, b->cmax[i]);
+            b->any_bytes = true;
+        }
+    }
+    b->tstride = cm_all + 1;
+    for (auto& g : b->graphs) {                             // resident cost vectors
+        const bool bytes = g.cmax != 0xffffffffu;
+        const idx_t dim = idx_t(1) << g.n;
+        unsigned char* d_e = nullptr;
+        double* d_w = nullptr;
+        if ((rc = (int)cudaMalloc(&g.d_cost, dim * (bytes ? 1 : 8))) || (rc = dalloc(&d_e, g.edges.size())) ||
+            (rc = dalloc(&d_w, g.w.size()))) {
+            cudaFree(d_e);
+            orkan_qaoa_destroy(b);
+            return rc;
+        }
+        if (!g.w.empty()) {
+            cudaMemcpy(d_e, g.edges.data(), g.edges.size(), cudaMemcpyHostToDevice);
+            cudaMemcpy(d_w, g.w.data(), g.w.size() * 8, cudaMemcpyHostToDevice);
+        }
+        const unsigned grid = (unsigned)std::min<idx_t>((dim + 255) / 256, (idx_t)sm_count() * 16);
+        if (bytes) k_qaoa_cost<uint8_t><<<grid, 256>>>((uint8_t*)g.d_cost, g.n, d_e, d_w, (unsigned)g.w.size());
+        else k_qaoa_cost<double><<<grid, 256>>>((double*)g.d_cost, g.n, d_e, d_w, (unsigned)g.w.size());
+        rc = (int)cudaGetLastError();
+        if (!rc) rc = (int)cudaDeviceSynchronize();
+        cudaFree(d_e);
+        cudaFree(d_w);
+        if (rc) {
+            orkan_qaoa_destroy(b);
+            return rc;
+        }
+    }
+    size_t freeb = 0, totalb = 0;
+    cudaMemGetInfo(&freeb, &totalb);
+    b->budget = mem_budget ? mem_budget : (unsigned long long)(0.6 * (double)freeb);
+    const size_t np = (size_t)count * p;
+    if ((rc = dalloc(&b->d_cmax, count)) || (rc = dalloc(&b->d_gamma, np)) || (rc = dalloc(&b->d_rx, np)) ||
+        (rc = dalloc(&b->d_table, b->any_bytes ? np * b->tstride : 1)) || (rc = dalloc(&b->d_out, count)) ||
+        (rc = (int)cudaMallocHost(&b->h_gamma, np * 8)) || (rc = (int)cudaMallocHost(&b->h_rx, np * 16)) ||
+        (rc = (int)cudaMallocHost(&b->h_out, (size_t)count * 8)) ||
+        (rc = (int)cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking))) {
+        orkan_qaoa_destroy(b);
+        return rc;
+    }
+    cudaMemcpy(b->d_cmax, b->cmax.data(), count * sizeof(unsigned), cudaMemcpyHostToDevice);
+    memset(b->h_gamma, 0, np * 8);
+    memset(b->h_rx, 0, np * 16);
+    if ((rc = rebuild(b))) {
+        orkan_qaoa_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return 0;
+}
+
+int orkan_qaoa_run(orkan_qaoa_t* b, const double* gammas, const double* betas, double* means, void* stream) {
+    if (!b || !gammas || !betas || !means) return (int)cudaErrorInvalidValue;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    int rc = (int)cudaStreamSynchronize(st);                // the staging buffers may still be read
+    if (rc) return rc;
+    stage_angles(b, gammas, betas);
+    if ((rc = (int)cudaGraphLaunch(b->exec, st))) return rc;
+    if ((rc = (int)cudaStreamSynchronize(st))) return rc;
+    memcpy(means, b->h_out, (size_t)b->count * 8);
+    return 0;
+}
+
+int orkan_qaoa_config(const orkan_qaoa_t* b, unsigned n, unsigned* log_chunk, unsigned* threads) {
+    if (!b || n > 26) return (int)cudaErrorInvalidValue;
+    if (log_chunk) *log_chunk = b->cfgC[n];
+    if (threads) *threads = b->cfgT[n];
+    return 0;
+}
+
+int orkan_qaoa_stats(const orkan_qaoa_t* b, unsigned* waves, unsigned* launches) {
+    if (!b) return (int)cudaErrorInvalidValue;
+    if (waves) *waves = b->plan.waves;
+    if (launches) *launches = (unsigned)b->plan.launches.size() + (b->any_bytes ? 1u : 0u);
+    return 0;
+}
+
+int orkan_qaoa_cost_vector(orkan_qaoa_t* b, unsigned i, double* host_out) {
+    if (!b || !host_out || i >= b->count) return (int)cudaErrorInvalidValue;
+    const Graph& g = b->graphs[b->gid[i]];
+    const idx_t dim = idx_t(1) << g.n;
+    if (g.cmax == 0xffffffffu) return (int)cudaMemcpy(host_out, g.d_cost, dim * 8, cudaMemcpyDeviceToHost);
+    std::vector<uint8_t> tmp(dim);
+    const int rc = (int)cudaMemcpy(tmp.data(), g.d_cost, dim, cudaMemcpyDeviceToHost);
+    for (idx_t x = 0; x < dim; ++x) host_out[x] = tmp[x];
+    return rc;
+}
+
+int orkan_qaoa_tune(orkan_qaoa_t* b, const double* gammas, const double* betas, const char* cache_path) {
+    if (!b || !gammas || !betas) return (int)cudaErrorInvalidValue;
+    std::vector<std::pair<unsigned, bool>> groups;          // distinct (qubit count, cost type)
+    for (unsigned i = 0; i < b->count; ++i) {
+        const auto key = std::make_pair(b->n[i], b->cmax[i] < kQaoaMaxTable);
+        if (std::find(groups.begin(), groups.end(), key) == groups.end()) groups.push_back(key);
+    }
+    std::string cached;
+    if (cache_path) {
+        if (FILE* f = fopen(cache_path, "r")) {
+            char line[512];
+            while (fgets(line, sizeof line, f)) cached += line;
+            fclose(f);
+        }
+    }
+    stage_angles(b, gammas, betas);
+    const size_t np = (size_t)b->count * b->p;
+    int rc;
+    if ((rc = (int)cudaMemcpyAsync(b->d_gamma, b->h_gamma, np * 8, cudaMemcpyHostToDevice, b->cap)) ||
+        (rc = (int)cudaMemcpyAsync(b->d_rx, b->h_rx, np * 16, cudaMemcpyHostToDevice, b->cap)) ||
+        (rc = enqueue_tables(b, b->cap)) || (rc = (int)cudaStreamSynchronize(b->cap)))
+        return rc;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::string append;
+    for (const auto& grp : groups) {
+        const unsigned nq = grp.first;
+        const std::string key = cache_key(b, nq, grp.second);
+        const size_t at = cached.find("\"" + key + "\"");
+        unsigned C = 0, t = 0;
+        if (at != std::string::npos &&
+            sscanf(cached.c_str() + at + key.size() + 2, ": {\"C\": %u, \"threads\": %u", &C, &t) == 2 &&
+            C <= kQaoaMaxC && (C >= nq || 2 * C >= nq) && (t == 256 || t == 512)) {
+            b->cfgC[nq] = C;
+            b->cfgT[nq] = t;
+            continue;
+        }
+        // up to 64 instances of the group, within one wave's budget
+        std::vector<unsigned> sel;
+        size_t bytes = 0;
+        for (unsigned i = 0; i < b->count && sel.size() < 64; ++i)
+            if (b->n[i] == nq && (b->cmax[i] < kQaoaMaxTable) == grp.second) {
+                if (!sel.empty() && bytes + (size_t(1) << nq) * 16 > b->budget) break;
+                bytes += (size_t(1) << nq) * 16;
+                sel.push_back(i);
+            }
+        float best = 1e30f;
+        unsigned bestC = b->cfgC[nq], bestT = b->cfgT[nq];
+        const unsigned c_lo = std::min(kQaoaMaxC, std::max(10u, (nq + 1) / 2));
+        for (unsigned Cc = c_lo; Cc <= kQaoaMaxC; ++Cc) {
+            for (unsigned tt : {256u, 512u}) {
+                b->cfgC[nq] = Cc;
+                b->cfgT[nq] = tt;
+                Plan pl = make_plan(b, sel);
+                if (upload_plan(b, pl)) { cudaGetLastError(); continue; }
+                if (enqueue_kernels(b, pl, b->cap)) { cudaGetLastError(); continue; }   // warm-up
+                cudaEventRecord(e0, b->cap);
+                bool ok = true;
+                for (int r = 0; r < 3 && ok; ++r) ok = enqueue_kernels(b, pl, b->cap) == 0;
+                cudaEventRecord(e1, b->cap);
+                if (!ok || cudaEventSynchronize(e1) != cudaSuccess) { cudaGetLastError(); continue; }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best) { best = ms; bestC = Cc; bestT = tt; }
+            }
+            if (Cc >= nq) break;                            // a full pass: larger chunks change nothing
+        }
+        b->cfgC[nq] = bestC;
+        b->cfgT[nq] = bestT;
+        char line[512];
+        snprintf(line, sizeof line, "{\"%s\": {\"C\": %u, \"threads\": %u, \"ms_per_instance\": %.5f}}\n", key.c_str(),
+                 bestC, bestT, best / 3 / (sel.empty() ? 1 : sel.size()));
+        append += line;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (cache_path && !append.empty()) {
+        if (FILE* f = fopen(cache_path, "a")) {
+            fputs(append.c_str(), f);
+            fclose(f);
+        }
+    }
+    return rebuild(b);
+}
+
+void orkan_qaoa_destroy(orkan_qaoa_t* b) {
+    if (!b) return;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    for (auto& g : b->graphs) cudaFree(g.d_cost);
+    cudaFree(b->d_cmax);
+    cudaFree(b->d_gamma);
+    cudaFree(b->d_rx);
+    cudaFree(b->d_table);
+    cudaFree(b->d_out);
+    cudaFree(b->d_partial);
+    cudaFree(b->d_arena);
+    cudaFree(b->d_inst);
+    cudaFreeHost(b->h_gamma);
+    cudaFreeHost(b->h_rx);
+    cudaFreeHost(b->h_out);
+    delete b;
+}
+
+}  // extern "C"

@@ -12,6 +12,7 @@
 #include "../../orkan_b200/csrc/cuda/dm_engine.cuh"
 #include "../../orkan_b200/csrc/cuda/dm_phase.cuh"
 #include "../../orkan_b200/csrc/cuda/pure.cuh"
+#include "../../orkan_b200/csrc/cuda/qaoa.cuh"
 
 #include <stdint.h>
 #include <stdlib.h>
@@ -76,6 +77,17 @@ struct EmuMemC2 {
     }
 };
 
+template <class CostT>
+struct EmuCost {
+    const CostT* p;
+    idx_t len;
+    uint64_t* oob;
+    CostT ld(idx_t i) const {
+        if (i >= len) { ++*oob; return CostT(0); }
+        return p[i];
+    }
+};
+
 constexpr unsigned kSms = 148;
 
 unsigned grid_for(idx_t per_block, idx_t total, unsigned cap) {
@@ -136,6 +148,70 @@ void run_phase(int layout, unsigned log_tile, const EmuMem& mem, unsigned n, con
                 if (layout == 1) dm_phase_item(mem, PackedMap{idx_t(1) << n}, g, fac, w, t, kPhaseThreads);
                 else dm_phase_item(mem, TiledMap{idx_t(1) << n, log_tile}, g, fac, w, t, kPhaseThreads);
             }
+}
+
+
+// One instance through the fused QAOA passes 0..upto (the GPU launch plan with a single
+// instance): full pass when n <= C, else p + 1 low/high passes of 2^C-amplitude chunks.
+template <class CostT>
+int run_qaoa(unsigned n, const CostT* cost, unsigned p, const double* gamma, const double* beta, unsigned C,
+             unsigned nthr, unsigned upto, double* psi, double* mean, uint32_t* reads, uint32_t* writes,
+             uint64_t* oob) {
+    const bool full = n <= C;
+    if (p == 0 || nthr % 32 || (!full && 2 * C < n) || C > kQaoaMaxC) return -1;
+    const idx_t dim = idx_t(1) << n;
+    std::vector<double2> rx(p), table(1, c2(1.0, 0.0));
+    unsigned tstride = 1;
+    for (unsigned k = 0; k < p; ++k) rx[k] = c2(cos(2.0 * beta[k] / 2.0), sin(2.0 * beta[k] / 2.0));
+    if (sizeof(CostT) == 1) {
+        unsigned cmax = 0;
+        for (idx_t x = 0; x < dim; ++x) cmax = cost[x] > cmax ? (unsigned)cost[x] : cmax;
+        tstride = cmax + 1;
+        table.assign((size_t)p * tstride, c2(0.0, 0.0));
+        for (unsigned k = 0; k < p; ++k)
+            for (unsigned c = 0; c <= cmax; ++c) {
+                double sn, cs;
+                sincos((double)c * gamma[k], &sn, &cs);
+                table[(size_t)k * tstride + c] = c2(cs, sn);
+            }
+    }
+    QaoaInst I;
+    I.psi = reinterpret_cast<double2*>(psi);
+    I.cost = cost;
+    I.item0 = 0;
+    I.n = n;
+    I.pos = 0;
+    const EmuMem mem{reinterpret_cast<double2*>(psi), dim, reads, writes, oob};
+    const EmuCost<CostT> cmem{cost, dim, oob};
+    const unsigned npass = full ? 1 : p + 1;
+    for (unsigned j = 0; j < npass && j <= upto; ++j) {
+        QaoaPass P;
+        P.inst = &I;
+        P.ninst = 1;
+        P.kind = full ? kQaoaFull : ((j % 2 == 0) ? kQaoaLow : kQaoaHigh);
+        P.C = full ? n : C;
+        P.items = qaoa_items(n, P.C, P.kind);
+        P.gamma = gamma;
+        std::vector<double> partial(P.items, 0.0);
+        P.partial = partial.data();
+        P.p = p;
+        P.pass = full ? 0 : j;
+        const QaoaTables T{table.data(), rx.data(), tstride};
+        const QaoaPlan pl = qaoa_plan(n, P.C, P.kind, p, P.pass);
+        std::vector<double2> vb(size_t(1) << P.C);
+        std::vector<double> red(nthr + 32);
+        std::vector<CostT> cb(size_t(1) << P.C);
+        const QaoaSmem<CostT> S{vb.data(), red.data(), cb.data()};
+        for (idx_t w = 0; w < P.items; ++w)
+            for (unsigned st = 0; st < qaoa_stages(pl); ++st)
+                for (unsigned t = 0; t < nthr; ++t) qaoa_stage<CostT>(P, T, I, pl, mem, cmem, w, st, S, t, nthr);
+        if (pl.measure) {
+            double s = 0.0;
+            for (idx_t w = 0; w < P.items; ++w) s += partial[w];
+            *mean = s;
+        }
+    }
+    return 0;
 }
 
 }  // namespace
@@ -287,6 +363,14 @@ int emu_fill(double* data, uint64_t len, double re, double im, unsigned corner_l
     EmuMem mem{reinterpret_cast<double2*>(data), len, reads, writes, oob};
     for (idx_t tid = 0; tid < nthr; ++tid) fill_thread(mem, len, c2(re, im), corner_log_tile, corner_dim, tid, nthr);
     return 0;
+}
+
+// Fused QAOA passes of one instance; byte_cost selects byte costs (cost_b) over doubles.
+int emu_qaoa(unsigned n, const double* cost_d, const uint8_t* cost_b, int byte_cost, unsigned p, const double* gamma,
+             const double* beta, unsigned C, unsigned nthr, unsigned upto, double* psi, double* mean,
+             uint32_t* reads, uint32_t* writes, uint64_t* oob) {
+    if (byte_cost) return run_qaoa<uint8_t>(n, cost_b, p, gamma, beta, C, nthr, upto, psi, mean, reads, writes, oob);
+    return run_qaoa<double>(n, cost_d, p, gamma, beta, C, nthr, upto, psi, mean, reads, writes, oob);
 }
 
 }  // extern "C"

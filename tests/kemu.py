@@ -20,7 +20,7 @@ LAYOUT = {"pure": 0, "packed": 1, "tiled": 2}
 def build() -> str:
     src = os.path.join(HERE, "emu", "emu.cpp")
     deps = [src] + [os.path.join(HERE, "..", "orkan_b200", "csrc", "cuda", f)
-                    for f in ("common.cuh", "dm_engine.cuh", "dm_phase.cuh", "pure.cuh")]
+                    for f in ("common.cuh", "dm_engine.cuh", "dm_phase.cuh", "pure.cuh", "qaoa.cuh")]
     if not os.path.exists(LIB) or any(os.path.getmtime(d) > os.path.getmtime(LIB) for d in deps):
         import subprocess
         cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
@@ -173,3 +173,18 @@ def dm_gate(layout, lt, data, n, name, qubits, theta=None):
     if name == "ccx":
         return dm_monomial(layout, lt, data, n, q, [0, 1, 2, 3, 4, 5, 7, 6], [1] * 8)
     raise ValueError(name)
+
+
+def qaoa(n, cost, p, gammas, betas, log_chunk, nthr=64, upto=None, byte_cost=False):
+    """Fused QAOA passes 0..upto of one instance; returns (Result over psi, mean or None)."""
+    dim = 1 << n
+    cd = _arr(cost, np.float64)
+    cb = _arr(np.asarray(cost), np.uint8) if byte_cost else np.zeros(1, np.uint8)
+    g = _arr(gammas, np.float64)
+    bt = _arr(betas, np.float64)
+    mean = C.c_double(float("nan"))
+    up = p if upto is None else upto
+    res = _run(lib().emu_qaoa, np.zeros(dim, dtype=np.complex128),
+               lambda o, r, w, b: (n, _ptr(cd), _ptr(cb), int(byte_cost), p, _ptr(g), _ptr(bt), log_chunk, nthr, up,
+                                   _ptr(o), C.byref(mean), _ptr(r), _ptr(w), C.byref(b)))
+    return res, (None if np.isnan(mean.value) else mean.value)

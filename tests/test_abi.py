@@ -135,3 +135,32 @@ print("data", s.data, "qubits", s.qubits)
     assert r.returncode == 0, r.stderr
     assert "data None qubits 0" in r.stdout
     assert "state_init(): device allocation failed" in r.stderr
+
+
+def test_batch_entry_points_declared_and_validate_without_gpu():
+    """orkan_batch.h: every entry point is exported, and orkan_qaoa_create rejects invalid
+    batches (cudaErrorInvalidValue = 1) before touching a device."""
+    from orkan_b200.build import library_path
+    decl = declared_functions()
+    for f in ("create", "run", "tune", "config", "cost_vector", "stats", "destroy"):
+        assert "orkan_qaoa_" + f in decl
+    lib = C.CDLL(library_path(5))
+    lib.orkan_qaoa_create.argtypes = [C.POINTER(C.c_void_p), C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_uint, C.c_ulonglong, C.c_uint]
+    import numpy as np
+
+    def create(ns, edges, offs, p=2):
+        ns = np.asarray(ns, np.uint32)
+        ed = np.asarray(edges if edges else [0], np.uint32)
+        of = np.asarray(offs, np.uint32)
+        h = C.c_void_p(1)
+        rc = lib.orkan_qaoa_create(C.byref(h), len(ns), ns.ctypes.data, of.ctypes.data, ed.ctypes.data, None, p,
+                                   0, 0)
+        return rc, h.value
+
+    assert create([27], [], [0, 0]) == (1, None)            # more than 26 qubits
+    assert create([0], [], [0, 0]) == (1, None)             # no qubits
+    assert create([4], [0, 4], [0, 1]) == (1, None)         # vertex out of range
+    assert create([4], [2, 2], [0, 1]) == (1, None)         # self loop
+    assert create([4], [0, 1], [0, 1], p=0) == (1, None)    # no layers
+    assert create([4, 4], [0, 1], [0, 1, 0]) == (1, None)   # decreasing offsets
