@@ -52,12 +52,11 @@ __global__ void k_qaoa_tables(const unsigned* cmax, const double* gamma, unsigne
 }
 
 template <unsigned NT, class CostT>
-__global__ void __launch_bounds__(NT) k_qaoa_pass(QaoaPass P, QaoaTables T) {
+__global__ void __launch_bounds__(NT, NT == 128 ? 3 : 512 / NT) k_qaoa_pass(QaoaPass P, QaoaTables T) {
     extern __shared__ double2 smem_q[];
-    QaoaSmem<CostT> S;
+    QaoaSmem S;
     S.vb = smem_q;
     S.red = reinterpret_cast<double*>(smem_q + (1u << P.C));
-    S.cb = reinterpret_cast<CostT*>(S.red + NT + 32);
     for (idx_t w = blockIdx.x; w < P.items; w += gridDim.x) {
         const QaoaInst I = P.inst[qaoa_find(P.inst, P.ninst, w)];
         const QaoaPlan pl = qaoa_plan(I.n, P.C, P.kind, P.p, P.pass);
@@ -109,14 +108,16 @@ int pass_grid(size_t smem, idx_t items, unsigned* grid) {
 // (Called before any graph capture: it sets the kernel's shared-memory attribute.)
 template <class CostT>
 int pass_grid_t(unsigned nt, unsigned C, idx_t items, unsigned* grid) {
-    const size_t smem = qaoa_smem_bytes<CostT>(C, nt);
+    const size_t smem = qaoa_smem_bytes(C, nt);
+    if (nt == 128) return pass_grid<128, CostT>(smem, items, grid);
     return nt == 256 ? pass_grid<256, CostT>(smem, items, grid) : pass_grid<512, CostT>(smem, items, grid);
 }
 
 template <class CostT>
 int launch_pass_t(unsigned nt, unsigned grid, const QaoaPass& P, const QaoaTables& T, cudaStream_t st) {
-    const size_t smem = qaoa_smem_bytes<CostT>(P.C, nt);
-    if (nt == 256) k_qaoa_pass<256, CostT><<<grid, 256, smem, st>>>(P, T);
+    const size_t smem = qaoa_smem_bytes(P.C, nt);
+    if (nt == 128) k_qaoa_pass<128, CostT><<<grid, 128, smem, st>>>(P, T);
+    else if (nt == 256) k_qaoa_pass<256, CostT><<<grid, 256, smem, st>>>(P, T);
     else k_qaoa_pass<512, CostT><<<grid, 512, smem, st>>>(P, T);
     return (int)cudaGetLastError();
 }
@@ -162,7 +163,7 @@ struct orkan_qaoa {
     // device buffers
     unsigned* d_cmax = nullptr;
     double* d_gamma = nullptr;          // [instance][p]
-    double2* d_rx = nullptr;
+    QaoaRx* d_rx = nullptr;
     double2* d_table = nullptr;         // [instance][p][tstride]
     double* d_out = nullptr;
     double* d_partial = nullptr;
@@ -172,7 +173,7 @@ struct orkan_qaoa {
     size_t inst_cap = 0;
     // pinned host staging
     double* h_gamma = nullptr;
-    double2* h_rx = nullptr;
+    QaoaRx* h_rx = nullptr;
     double* h_out = nullptr;
     Plan plan;
     cudaStream_t cap = nullptr;
@@ -186,7 +187,7 @@ int dalloc(T** p, size_t count) {
     return (int)cudaMalloc(reinterpret_cast<void**>(p), (count ? count : 1) * sizeof(T));
 }
 
-unsigned default_C(unsigned n) { return n <= kQaoaMaxC ? n : kQaoaMaxC; }
+unsigned default_C(unsigned n) { return n <= 12 ? n : std::max(12u, (n + 1) / 2); }
 bool is_full(const orkan_qaoa* b, unsigned n) { return n <= b->cfgC[n]; }
 size_t state_bytes(const orkan_qaoa* b, unsigned n) { return is_full(b, n) ? 0 : (size_t(1) << n) * 16; }
 
@@ -331,7 +332,7 @@ int enqueue_run(const orkan_qaoa* b, const Plan& pl, cudaStream_t st) {
     const size_t np = (size_t)b->count * b->p;
     int rc;
     if ((rc = (int)cudaMemcpyAsync(b->d_gamma, b->h_gamma, np * 8, cudaMemcpyHostToDevice, st))) return rc;
-    if ((rc = (int)cudaMemcpyAsync(b->d_rx, b->h_rx, np * 16, cudaMemcpyHostToDevice, st))) return rc;
+    if ((rc = (int)cudaMemcpyAsync(b->d_rx, b->h_rx, np * sizeof(QaoaRx), cudaMemcpyHostToDevice, st))) return rc;
     if ((rc = enqueue_tables(b, st))) return rc;
     if ((rc = enqueue_kernels(b, pl, st))) return rc;
     return (int)cudaMemcpyAsync(b->h_out, b->d_out, (size_t)b->count * 8, cudaMemcpyDeviceToHost, st);
@@ -369,7 +370,7 @@ void stage_angles(orkan_qaoa* b, const double* gammas, const double* betas) {
     for (size_t k = 0; k < np; ++k) {
         const double theta = 2.0 * betas[k];
         b->h_gamma[k] = gammas[k];
-        b->h_rx[k] = c2(cos(theta / 2.0), sin(theta / 2.0));
+        b->h_rx[k] = qaoa_rx_coeffs(cos(theta / 2.0), sin(theta / 2.0));
     }
 }
 
@@ -404,7 +405,7 @@ int orkan_qaoa_create(orkan_qaoa_t** out, unsigned count, const unsigned* n_qubi
     b->n.assign(n_qubits, n_qubits + count);
     for (unsigned q = 0; q <= 26; ++q) {
         b->cfgC[q] = default_C(q);
-        b->cfgT[q] = 512;
+        b->cfgT[q] = 128;
     }
     // distinct graphs (same qubit count, edges in the same order, same weights)
     std::map<std::vector<unsigned char>, unsigned> seen;
@@ -480,7 +481,7 @@ int orkan_qaoa_create(orkan_qaoa_t** out, unsigned count, const unsigned* n_qubi
     const size_t np = (size_t)count * p;
     if ((rc = dalloc(&b->d_cmax, count)) || (rc = dalloc(&b->d_gamma, np)) || (rc = dalloc(&b->d_rx, np)) ||
         (rc = dalloc(&b->d_table, b->any_bytes ? np * b->tstride : 1)) || (rc = dalloc(&b->d_out, count)) ||
-        (rc = (int)cudaMallocHost(&b->h_gamma, np * 8)) || (rc = (int)cudaMallocHost(&b->h_rx, np * 16)) ||
+        (rc = (int)cudaMallocHost(&b->h_gamma, np * 8)) || (rc = (int)cudaMallocHost(&b->h_rx, np * sizeof(QaoaRx))) ||
         (rc = (int)cudaMallocHost(&b->h_out, (size_t)count * 8)) ||
         (rc = (int)cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking))) {
         orkan_qaoa_destroy(b);
@@ -488,7 +489,7 @@ int orkan_qaoa_create(orkan_qaoa_t** out, unsigned count, const unsigned* n_qubi
     }
     cudaMemcpy(b->d_cmax, b->cmax.data(), count * sizeof(unsigned), cudaMemcpyHostToDevice);
     memset(b->h_gamma, 0, np * 8);
-    memset(b->h_rx, 0, np * 16);
+    memset(b->h_rx, 0, np * sizeof(QaoaRx));
     if ((rc = rebuild(b))) {
         orkan_qaoa_destroy(b);
         return rc;
@@ -553,7 +554,7 @@ int orkan_qaoa_tune(orkan_qaoa_t* b, const double* gammas, const double* betas, 
     const size_t np = (size_t)b->count * b->p;
     int rc;
     if ((rc = (int)cudaMemcpyAsync(b->d_gamma, b->h_gamma, np * 8, cudaMemcpyHostToDevice, b->cap)) ||
-        (rc = (int)cudaMemcpyAsync(b->d_rx, b->h_rx, np * 16, cudaMemcpyHostToDevice, b->cap)) ||
+        (rc = (int)cudaMemcpyAsync(b->d_rx, b->h_rx, np * sizeof(QaoaRx), cudaMemcpyHostToDevice, b->cap)) ||
         (rc = enqueue_tables(b, b->cap)) || (rc = (int)cudaStreamSynchronize(b->cap)))
         return rc;
     cudaEvent_t e0, e1;
@@ -567,7 +568,7 @@ int orkan_qaoa_tune(orkan_qaoa_t* b, const double* gammas, const double* betas, 
         unsigned C = 0, t = 0;
         if (at != std::string::npos &&
             sscanf(cached.c_str() + at + key.size() + 2, ": {\"C\": %u, \"threads\": %u", &C, &t) == 2 &&
-            C <= kQaoaMaxC && (C >= nq || 2 * C >= nq) && (t == 256 || t == 512)) {
+            C <= kQaoaMaxC && (C >= nq || 2 * C >= nq) && (t == 128 || t == 256 || t == 512)) {
             b->cfgC[nq] = C;
             b->cfgT[nq] = t;
             continue;
@@ -585,7 +586,7 @@ int orkan_qaoa_tune(orkan_qaoa_t* b, const double* gammas, const double* betas, 
         unsigned bestC = b->cfgC[nq], bestT = b->cfgT[nq];
         const unsigned c_lo = std::min(kQaoaMaxC, std::max(10u, (nq + 1) / 2));
         for (unsigned Cc = c_lo; Cc <= kQaoaMaxC; ++Cc) {
-            for (unsigned tt : {256u, 512u}) {
+            for (unsigned tt : {128u, 256u, 512u}) {
                 b->cfgC[nq] = Cc;
                 b->cfgT[nq] = tt;
                 Plan pl = make_plan(b, sel);

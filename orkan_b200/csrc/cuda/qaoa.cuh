@@ -11,27 +11,34 @@
 //     pass 0 (low):           init, D1, L1
 //     pass j (1 <= j < p):    Mix_j, D_{j+1}, Mix_{j+1}   with Mix = H (j odd) or L (j even)
 //     pass p:                 Mix_p, M
-// and each pass touches every amplitude once: a low pass stages 2^C contiguous amplitudes,
-// a high pass stages W = 2^(2C - n) neighbouring columns of all 2^(n - C) rows (x = row *
-// 2^C + col), so the qubits it mixes are local in both.  Instances with n <= C run the
-// whole circuit in one pass ("full") and never touch a state vector in device memory.
+// and each pass touches every amplitude once: a low pass works on chunks of 2^C contiguous
+// amplitudes, a high pass on W = 2^(2C - n) neighbouring columns of all 2^(n - C) rows
+// (x = row * 2^C + col), so the qubits it mixes are local in both.  Instances with n <= C
+// run the whole circuit in one pass ("full") and never touch a state vector in memory.
 //
-// Inside a work item the staged chunk lives in shared memory; the mixer runs in register
-// stages of up to kQaoaGroup qubits each (every thread holds 2^k amplitudes that differ
-// only in the group's bits and applies the group's butterflies in registers).  Rx on
-// different qubits commute, so segment t + 1 starts with the group segment t ended with;
-// that stage applies segment t's butterflies, the phase between the segments and
-// segment t + 1's butterflies without going back to shared memory.
+// Inside a work item the mixer runs in register stages of up to kQaoaGroup qubits (every
+// thread holds 2^k amplitudes that differ only in the group's bits and applies the group's
+// butterflies in registers); between stages the chunk sits in shared memory.  Rx on
+// different qubits commute, so the order of the groups is free: the first stage of a pass
+// loads its amplitudes straight from device memory and the last one stores them (or
+// measures), both with a group whose bits exclude the low slot bits, so that consecutive
+// lanes touch consecutive amplitudes; and segment t + 1 starts with the group segment t
+// ended with, so that stage applies segment t's butterflies, the phase between the
+// segments and segment t + 1's butterflies without going back to shared memory.
 //
-// Arithmetic matches the per-call path: rx uses the pair formula of gate_pure.c with
-// c = cos(beta), s = sin(beta) (rx(2 beta) takes cos(2 beta / 2), the same value); the
+// Arithmetic (checked against the per-call path at 1e-12): the rx pair update
+// (a, b) -> (c a - i s b, c b - i s a) with c = cos(beta), s = sin(beta) (rx(2 beta) of
+// gate_pure.c) is applied as k-form (a - i t b, b - i t a), t = s / c, when |c| >= |s|, or as
+// (u a - i b, u b - i a), u = c / s, otherwise -- four FMAs per pair -- and the product of
+// the dropped factors (c or s, once per qubit) scales each amplitude once per segment; the
 // phase is (c re + s im, c im - s re) with (s, c) = sincos(cost[x] * gamma) (taken from a
-// per-layer table, made by the same sincos, when the costs are stored as bytes); the mean
-// is sum cost[x] |psi_x|^2, in a fixed order per chunk.
+// per-layer table, made by the same sincos, when the costs are stored as bytes); the mean is
+// sum cost[x] |psi_x|^2 in a fixed order per chunk.
 #pragma once
 
 #include "common.cuh"
-#include "pure.cuh"
+
+#include <math.h>
 
 #include <type_traits>
 
@@ -59,13 +66,31 @@ struct QaoaPass {
     double* partial;       // measuring pass: one partial sum per work item
     unsigned p;
     unsigned pass;         // j in [0, p] (0 for full passes)
-    unsigned C;            // log2 of the chunk (amplitudes staged per item)
+    unsigned C;            // log2 of the chunk (amplitudes per item)
     unsigned kind;         // QaoaKind
 };
 
+// The mixer of one layer in the four-FMA form: k, the dropped factor, and which form.
+struct QaoaRx {
+    double k;
+    double scale;
+    int sform;             // 0: (a - i k b) with k = s / c, scale = c; 1: (k a - i b), k = c / s, scale = s
+    int pad_;
+};
+
+// Host side: the mixer coefficients of rx(theta) = exp(-i theta X / 2) from c = cos(theta / 2),
+// s = sin(theta / 2).
+inline QaoaRx qaoa_rx_coeffs(double c, double s) {
+    QaoaRx r;
+    if (fabs(c) >= fabs(s)) { r.k = s / c; r.scale = c; r.sform = 0; }
+    else { r.k = c / s; r.scale = s; r.sform = 1; }
+    r.pad_ = 0;
+    return r;
+}
+
 struct QaoaTables {
     const double2* phase;  // [pos][layer][tstride]: (cos, sin)(c * gamma) for byte costs c
-    const double2* rx;     // [pos][layer]: (cos(beta), sin(beta)) as the host computes them
+    const QaoaRx* rx;      // [pos][layer]
     unsigned tstride;
 };
 
@@ -73,12 +98,12 @@ struct QaoaTables {
 ORKAN_HD idx_t qaoa_items(unsigned n, unsigned C, unsigned kind) {
     return kind == kQaoaFull ? idx_t(1) : idx_t(1) << (n - C);
 }
-// log2 of the staged amplitudes of one item
+// log2 of the amplitudes of one item
 ORKAN_HD unsigned qaoa_lc(unsigned n, unsigned C, unsigned kind) { return kind == kQaoaFull ? n : C; }
 // log2 of the number of columns a high chunk spans
 ORKAN_HD unsigned qaoa_logw(unsigned n, unsigned C) { return 2 * C - n; }
 
-// Global amplitude index of staged slot s of chunk c.
+// Global amplitude index of slot s of chunk c.
 ORKAN_HD idx_t qaoa_index(unsigned n, unsigned C, unsigned kind, idx_t c, unsigned s) {
     if (kind == kQaoaFull) return s;
     if (kind == kQaoaLow) return (c << C) + s;
@@ -87,7 +112,12 @@ ORKAN_HD idx_t qaoa_index(unsigned n, unsigned C, unsigned kind, idx_t c, unsign
     return ((idx_t)row << C) + (c << lw) + col;
 }
 
-// Staged-slot bit of qubit q.
+// Index distance of slot bit b (a mixer qubit's bit: a row bit in high passes).
+ORKAN_HD idx_t qaoa_stride(unsigned n, unsigned C, unsigned kind, unsigned b) {
+    return kind == kQaoaHigh ? idx_t(1) << (b - qaoa_logw(n, C) + C) : idx_t(1) << b;
+}
+
+// Slot bit of qubit q.
 ORKAN_HD unsigned qaoa_bit(unsigned n, unsigned C, unsigned kind, unsigned q) {
     return kind == kQaoaHigh ? q - C + qaoa_logw(n, C) : q;
 }
@@ -103,19 +133,19 @@ ORKAN_HD unsigned qaoa_find(const QaoaInst* inst, unsigned ninst, idx_t w) {
     return lo;
 }
 
-// Shared-memory slot permutations that keep the register stages free of bank conflicts
-// for every group position (16-byte amplitudes, 8- and 1-byte costs).
+// Shared-memory slot permutation that keeps the register stages free of bank conflicts
+// for every group position (16-byte amplitudes).
 ORKAN_HD unsigned qaoa_sw16(unsigned s) { return s ^ ((s >> 4) & 7u); }
-ORKAN_HD unsigned qaoa_sw8(unsigned s) { return s ^ ((s >> 4) & 15u); }
 
 // What one pass does.
 struct QaoaPlan {
     unsigned segs;             // mixer segments (1 or 2, or p for the full pass)
     unsigned q0, q1;           // qubit range of every segment
     unsigned layer0;           // layer of segment 0 (0-based); segment t is layer0 + t
-    int phase_load;            // layer whose phase follows the load (-1: none)
-    int init;                  // the load stage generates |+> instead of reading psi
+    int phase_load;            // layer whose phase precedes segment 0 (-1: none)
+    int init;                  // the pass starts from |+> instead of reading psi
     int measure;               // the pass ends with the mean instead of a store
+    int shape;                 // group orders: 0 full (rotating), 1 first pass, 2 middle, 3 last
     unsigned m;                // register groups per segment
     unsigned nreg;             // register stages
 };
@@ -126,13 +156,13 @@ ORKAN_HD QaoaPlan qaoa_plan(unsigned n, unsigned C, unsigned kind, unsigned p, u
     else if (kind == kQaoaLow) { pl.q0 = 0; pl.q1 = C; }
     else { pl.q0 = C; pl.q1 = n; }
     if (kind == kQaoaFull) {            // init, D1, Mix1, D2, Mix2, ..., Dp, Mixp, measure
-        pl.segs = p; pl.layer0 = 0; pl.phase_load = 0; pl.init = 1; pl.measure = 1;
+        pl.segs = p; pl.layer0 = 0; pl.phase_load = 0; pl.init = 1; pl.measure = 1; pl.shape = 0;
     } else if (j == 0) {                // init, D1, Mix1
-        pl.segs = 1; pl.layer0 = 0; pl.phase_load = 0; pl.init = 1; pl.measure = 0;
+        pl.segs = 1; pl.layer0 = 0; pl.phase_load = 0; pl.init = 1; pl.measure = 0; pl.shape = 1;
     } else if (j < p) {                 // Mix_j, D_{j+1}, Mix_{j+1}  (0-based layers j-1, j)
-        pl.segs = 2; pl.layer0 = j - 1; pl.phase_load = -1; pl.init = 0; pl.measure = 0;
+        pl.segs = 2; pl.layer0 = j - 1; pl.phase_load = -1; pl.init = 0; pl.measure = 0; pl.shape = 2;
     } else {                            // Mix_p, measure
-        pl.segs = 1; pl.layer0 = p - 1; pl.phase_load = -1; pl.init = 0; pl.measure = 1;
+        pl.segs = 1; pl.layer0 = p - 1; pl.phase_load = -1; pl.init = 0; pl.measure = 1; pl.shape = 3;
     }
     const unsigned nq = pl.q1 - pl.q0;
     pl.m = (nq + kQaoaGroup - 1) / kQaoaGroup;
@@ -140,19 +170,53 @@ ORKAN_HD QaoaPlan qaoa_plan(unsigned n, unsigned C, unsigned kind, unsigned p, u
     return pl;
 }
 
-// Stages of one work item: load, the register stages, then store (or two fold stages).
-ORKAN_HD unsigned qaoa_stages(const QaoaPlan& pl) { return 1 + pl.nreg + (pl.measure ? 2u : 1u); }
+// Stages of one work item: the register stages, then two fold stages when measuring.
+ORKAN_HD unsigned qaoa_stages(const QaoaPlan& pl) { return pl.nreg + (pl.measure ? 2u : 0u); }
 
-// Register stage r: group g, applied for segments t0..t1 (t1 = t0 + 1 when the stage
-// carries the phase between two segments; all segments when there is a single group).
-ORKAN_HD void qaoa_reg_stage(const QaoaPlan& pl, unsigned r, unsigned* g, unsigned* t0, unsigned* t1) {
-    if (pl.m == 1) { *g = 0; *t0 = 0; *t1 = pl.segs - 1; return; }
-    unsigned t, i;
-    if (r < pl.m) { t = 0; i = r; }
-    else { const unsigned k = r - pl.m; t = 1 + k / (pl.m - 1); i = 1 + k % (pl.m - 1); }
-    *g = (i + pl.m - (t % pl.m)) % pl.m;
-    *t0 = t;
-    *t1 = (i == pl.m - 1 && t + 1 < pl.segs) ? t + 1 : t;
+// Group at position i of segment t's order.  Group m - 1 holds the highest slot bits; the
+// first pass ends with it (store), the last starts with it (load), a middle pass does both.
+ORKAN_HD unsigned qaoa_order(const QaoaPlan& pl, unsigned t, unsigned i) {
+    const unsigned m = pl.m;
+    switch (pl.shape) {
+        case 0: return (i + m - (t % m)) % m;
+        case 1: return i;
+        case 3: return i == 0 ? m - 1 : i - 1;
+        default:
+            if (t == 0) return i == 0 ? m - 1 : i - 1;
+            return i + 1 < m ? m - 2 - i : m - 1;
+    }
+}
+
+enum : unsigned { kQaoaFromSmem = 0, kQaoaFromGlobal = 1, kQaoaFromInit = 2 };
+enum : unsigned { kQaoaToSmem = 0, kQaoaToGlobal = 1, kQaoaToMeasure = 2 };
+
+struct QaoaStage {
+    unsigned g;                // group
+    unsigned t0, t1;           // segments applied in this stage
+    unsigned src, dst;
+    int pre_phase;             // phase of segment t0's preceding layer applied before it (-1: none)
+    int end0;                  // segment t0 ends in this stage (all of t0..t1 when there is one group)
+};
+
+// Register stage r of a pass.  Stages 0..m-1 run segment 0's groups; every later segment
+// adds m - 1 stages (its first group shares the previous segment's last stage).
+ORKAN_HD QaoaStage qaoa_reg_stage(const QaoaPlan& pl, unsigned r) {
+    QaoaStage s;
+    if (pl.m == 1) {
+        s.g = 0; s.t0 = 0; s.t1 = pl.segs - 1; s.end0 = 1;
+    } else {
+        unsigned t, i;
+        if (r < pl.m) { t = 0; i = r; }
+        else { const unsigned k = r - pl.m; t = 1 + k / (pl.m - 1); i = 1 + k % (pl.m - 1); }
+        s.g = qaoa_order(pl, t, i);
+        s.t0 = t;
+        s.t1 = (i == pl.m - 1 && t + 1 < pl.segs) ? t + 1 : t;
+        s.end0 = i == pl.m - 1;
+    }
+    s.src = r == 0 ? (pl.init ? kQaoaFromInit : kQaoaFromGlobal) : kQaoaFromSmem;
+    s.dst = r + 1 == pl.nreg ? (pl.measure ? kQaoaToMeasure : kQaoaToGlobal) : kQaoaToSmem;
+    s.pre_phase = (r == 0) ? pl.phase_load : -1;
+    return s;
 }
 
 ORKAN_HD double2 qaoa_apply_phase(double2 ph, double2 v) {
@@ -172,107 +236,154 @@ ORKAN_HD double2 qaoa_phase(CostT c, double gamma, const double2* table) {
     }
 }
 
-// Shared memory of one block: vb[2^C] amplitudes, red[nthr + 32] doubles, cb[2^C] costs.
-template <class CostT>
+// Shared memory of one block: vb[2^C] amplitudes, red[nthr + 32] doubles.
 struct QaoaSmem {
     double2* vb;
     double* red;
-    CostT* cb;
 };
 
-template <class CostT>
 ORKAN_HD size_t qaoa_smem_bytes(unsigned C, unsigned nthr) {
-    return (size_t(16) + sizeof(CostT)) * (size_t(1) << C) + size_t(8) * (nthr + 32);
+    return size_t(16) * (size_t(1) << C) + size_t(8) * (nthr + 32);
+}
+
+ORKAN_HD double qaoa_powu(double x, unsigned e) {
+    double r = 1.0;
+    for (unsigned i = 0; i < e; ++i) r *= x;
+    return r;
 }
 
 // Register stage of a group of K slot bits starting at b0.
-template <int K, class CostT>
+template <int K, class CostT, class Mem, class CostMem>
 ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst& I, const QaoaPlan& pl,
-                         const QaoaSmem<CostT>& S, unsigned lc, unsigned b0, unsigned t0, unsigned t1,
-                         bool measure, unsigned tid, unsigned nthr) {
+                         const QaoaStage& sg, const Mem& psi, const CostMem& cost, idx_t chunk,
+                         const QaoaSmem& S, unsigned lc, unsigned b0, unsigned tid, unsigned nthr) {
     constexpr unsigned NV = 1u << K;
+    const unsigned n = I.n;
     const unsigned sets = 1u << (lc - K);
     const unsigned lowm = (1u << b0) - 1;
+    const idx_t xs = qaoa_stride(n, P.C, P.kind, b0);
+    const unsigned nq = pl.q1 - pl.q0;
+    const idx_t row = (idx_t)I.pos * P.p;
+    const bool need_cost = sg.pre_phase >= 0 || sg.t1 > sg.t0 || sg.dst == kQaoaToMeasure;
+    const double amp0 = 1.0 / sqrt((double)(idx_t(1) << n));
     double acc = 0.0;
     for (unsigned r = tid; r < sets; r += nthr) {
         const unsigned base = (r & lowm) | ((r >> b0) << (b0 + K));
+        const idx_t xb = qaoa_index(n, P.C, P.kind, chunk, base);      // slot base | j << b0 is xb + j xs
         double2 v[NV];
+        CostT cv[NV];
+        if (sg.src == kQaoaFromGlobal) {
 #pragma unroll
-        for (unsigned j = 0; j < NV; ++j) v[j] = S.vb[qaoa_sw16(base | (j << b0))];
-        for (unsigned t = t0; t <= t1; ++t) {
+            for (unsigned j = 0; j < NV; ++j) v[j] = psi.ld(xb + j * xs);
+        } else if (sg.src == kQaoaFromSmem) {
+#pragma unroll
+            for (unsigned j = 0; j < NV; ++j) v[j] = S.vb[qaoa_sw16(base | (j << b0))];
+        } else {
+#pragma unroll
+            for (unsigned j = 0; j < NV; ++j) v[j] = c2(amp0, 0.0);
+        }
+        // byte costs are fetched with the amplitudes; FP64 costs (twice the registers) when
+        // first needed
+        bool have_cost = false;
+        auto fetch_cost = [&]() {
+            if (have_cost) return;
+#pragma unroll
+            for (unsigned j = 0; j < NV; ++j) cv[j] = cost.ld(xb + j * xs);
+            have_cost = true;
+        };
+        if (need_cost && (sizeof(CostT) == 1 || sg.pre_phase >= 0)) fetch_cost();
+        if (sg.pre_phase >= 0) {
+            const unsigned layer = pl.layer0 + (unsigned)sg.pre_phase;
+            const double gam = P.gamma[row + layer];
+            const double2* tb = T.phase + (row + layer) * T.tstride;
+#pragma unroll
+            for (unsigned j = 0; j < NV; ++j) v[j] = qaoa_apply_phase(qaoa_phase<CostT>(cv[j], gam, tb), v[j]);
+        }
+        for (unsigned t = sg.t0; t <= sg.t1; ++t) {
             const unsigned layer = pl.layer0 + t;
-            const double2 cs = T.rx[(idx_t)I.pos * P.p + layer];
+            const QaoaRx rx = T.rx[row + layer];
+            const double k = rx.k;
+            if (rx.sform == 0) {
 #pragma unroll
-            for (unsigned b = 0; b < (unsigned)K; ++b) {
+                for (unsigned b = 0; b < (unsigned)K; ++b)
 #pragma unroll
-                for (unsigned j = 0; j < NV; ++j)
-                    if (!(j & (1u << b))) pair_op<kOpRx>(v[j], v[j | (1u << b)], cs.x, cs.y);
+                    for (unsigned j = 0; j < NV; ++j)
+                        if (!(j & (1u << b))) {
+                            double2& a = v[j];
+                            double2& c = v[j | (1u << b)];
+                            const double2 na = c2(fma(k, c.y, a.x), fma(-k, c.x, a.y));
+                            c = c2(fma(k, a.y, c.x), fma(-k, a.x, c.y));
+                            a = na;
+                        }
+            } else {
+#pragma unroll
+                for (unsigned b = 0; b < (unsigned)K; ++b)
+#pragma unroll
+                    for (unsigned j = 0; j < NV; ++j)
+                        if (!(j & (1u << b))) {
+                            double2& a = v[j];
+                            double2& c = v[j | (1u << b)];
+                            const double2 na = c2(fma(k, a.x, c.y), fma(k, a.y, -c.x));
+                            c = c2(fma(k, c.x, a.y), fma(k, c.y, -a.x));
+                            a = na;
+                        }
             }
-            if (t < t1) {                                     // phase of the next layer
-                const double gam = P.gamma[(idx_t)I.pos * P.p + layer + 1];
-                const double2* tb = T.phase + ((idx_t)I.pos * P.p + layer + 1) * T.tstride;
+            const bool ends = (pl.m == 1) || (t == sg.t0 && sg.end0);
+            if (t < sg.t1) {                                  // scale of segment t, phase of the next layer
+                fetch_cost();
+                const double f = qaoa_powu(rx.scale, nq);
+                const double gam = P.gamma[row + layer + 1];
+                const double2* tb = T.phase + (row + layer + 1) * T.tstride;
 #pragma unroll
-                for (unsigned j = 0; j < NV; ++j)
-                    v[j] = qaoa_apply_phase(qaoa_phase<CostT>(S.cb[qaoa_sw8(base | (j << b0))], gam, tb), v[j]);
+                for (unsigned j = 0; j < NV; ++j) {
+                    const double2 ph = qaoa_phase<CostT>(cv[j], gam, tb);
+                    v[j] = qaoa_apply_phase(c2(ph.x * f, ph.y * f), v[j]);
+                }
+            } else if (ends) {
+                const double f = qaoa_powu(rx.scale, nq);
+#pragma unroll
+                for (unsigned j = 0; j < NV; ++j) v[j] = c2(v[j].x * f, v[j].y * f);
             }
         }
-        if (measure) {
+        if (sg.dst == kQaoaToMeasure) {
+            fetch_cost();
 #pragma unroll
-            for (unsigned j = 0; j < NV; ++j)
-                acc += (double)S.cb[qaoa_sw8(base | (j << b0))] * (v[j].x * v[j].x + v[j].y * v[j].y);
+            for (unsigned j = 0; j < NV; ++j) acc += (double)cv[j] * (v[j].x * v[j].x + v[j].y * v[j].y);
+        } else if (sg.dst == kQaoaToGlobal) {
+#pragma unroll
+            for (unsigned j = 0; j < NV; ++j) psi.st(xb + j * xs, v[j]);
         } else {
 #pragma unroll
             for (unsigned j = 0; j < NV; ++j) S.vb[qaoa_sw16(base | (j << b0))] = v[j];
         }
     }
-    if (measure) S.red[tid] = acc;
+    if (sg.dst == kQaoaToMeasure) S.red[tid] = acc;
 }
 
 // Per-thread work of stage `st` of one work item (instance I, chunk index `chunk`).
 // Barriers between the stages are the caller's.
 template <class CostT, class Mem, class CostMem>
 ORKAN_HD void qaoa_stage(const QaoaPass& P, const QaoaTables& T, const QaoaInst& I, const QaoaPlan& pl,
-                         const Mem& psi, const CostMem& cost, idx_t chunk, unsigned st, const QaoaSmem<CostT>& S,
+                         const Mem& psi, const CostMem& cost, idx_t chunk, unsigned st, const QaoaSmem& S,
                          unsigned tid, unsigned nthr) {
     const unsigned n = I.n, kind = P.kind;
-    const unsigned lc = qaoa_lc(n, P.C, kind);
-    const unsigned cnt = 1u << lc;
-    if (st == 0) {                                            // load (or |+>), costs, the load phase
-        const double amp = 1.0 / sqrt((double)(idx_t(1) << n));
-        const double gam = pl.phase_load >= 0 ? P.gamma[(idx_t)I.pos * P.p + (unsigned)pl.phase_load] : 0.0;
-        const double2* tb = T.phase + ((idx_t)I.pos * P.p + (pl.phase_load >= 0 ? pl.phase_load : 0)) * T.tstride;
-        for (unsigned s = tid; s < cnt; s += nthr) {
-            const idx_t x = qaoa_index(n, P.C, kind, chunk, s);
-            const CostT c = cost.ld(x);
-            double2 v = pl.init ? c2(amp, 0.0) : psi.ld(x);
-            if (pl.phase_load >= 0) v = qaoa_apply_phase(qaoa_phase<CostT>(c, gam, tb), v);
-            S.cb[qaoa_sw8(s)] = c;
-            S.vb[qaoa_sw16(s)] = v;
-        }
-        return;
-    }
-    if (st <= pl.nreg) {                                      // one register stage
-        unsigned g, t0, t1;
-        qaoa_reg_stage(pl, st - 1, &g, &t0, &t1);
+    if (st < pl.nreg) {
+        const QaoaStage sg = qaoa_reg_stage(pl, st);
+        const unsigned lc = qaoa_lc(n, P.C, kind);
         const unsigned nq = pl.q1 - pl.q0;
-        const unsigned off = g * kQaoaGroup;
+        const unsigned off = sg.g * kQaoaGroup;
         const unsigned k = (nq - off) < kQaoaGroup ? nq - off : kQaoaGroup;
         const unsigned b0 = qaoa_bit(n, P.C, kind, pl.q0 + off);
-        const bool measure = pl.measure && st == pl.nreg;
         switch (k) {
-            case 1: qaoa_group<1>(P, T, I, pl, S, lc, b0, t0, t1, measure, tid, nthr); break;
-            case 2: qaoa_group<2>(P, T, I, pl, S, lc, b0, t0, t1, measure, tid, nthr); break;
-            case 3: qaoa_group<3>(P, T, I, pl, S, lc, b0, t0, t1, measure, tid, nthr); break;
-            default: qaoa_group<4>(P, T, I, pl, S, lc, b0, t0, t1, measure, tid, nthr); break;
+            case 1: qaoa_group<1, CostT>(P, T, I, pl, sg, psi, cost, chunk, S, lc, b0, tid, nthr); break;
+            case 2: qaoa_group<2, CostT>(P, T, I, pl, sg, psi, cost, chunk, S, lc, b0, tid, nthr); break;
+            case 3: qaoa_group<3, CostT>(P, T, I, pl, sg, psi, cost, chunk, S, lc, b0, tid, nthr); break;
+            default: qaoa_group<4, CostT>(P, T, I, pl, sg, psi, cost, chunk, S, lc, b0, tid, nthr); break;
         }
-        return;
-    }
-    if (!pl.measure) {                                        // store
-        for (unsigned s = tid; s < cnt; s += nthr) psi.st(qaoa_index(n, P.C, kind, chunk, s), S.vb[qaoa_sw16(s)]);
         return;
     }
     // fold of the per-thread sums in a fixed order: 32 strided partial sums, then one
-    if (st == pl.nreg + 1) {
+    if (st == pl.nreg) {
         if (tid < 32) {
             double s = 0.0;
             for (unsigned t = tid; t < nthr; t += 32) s += S.red[t];

@@ -160,9 +160,10 @@ int run_qaoa(unsigned n, const CostT* cost, unsigned p, const double* gamma, con
     const bool full = n <= C;
     if (p == 0 || nthr % 32 || (!full && 2 * C < n) || C > kQaoaMaxC) return -1;
     const idx_t dim = idx_t(1) << n;
-    std::vector<double2> rx(p), table(1, c2(1.0, 0.0));
+    std::vector<QaoaRx> rx(p);
+    std::vector<double2> table(1, c2(1.0, 0.0));
     unsigned tstride = 1;
-    for (unsigned k = 0; k < p; ++k) rx[k] = c2(cos(2.0 * beta[k] / 2.0), sin(2.0 * beta[k] / 2.0));
+    for (unsigned k = 0; k < p; ++k) rx[k] = qaoa_rx_coeffs(cos(2.0 * beta[k] / 2.0), sin(2.0 * beta[k] / 2.0));
     if (sizeof(CostT) == 1) {
         unsigned cmax = 0;
         for (idx_t x = 0; x < dim; ++x) cmax = cost[x] > cmax ? (unsigned)cost[x] : cmax;
@@ -200,8 +201,7 @@ int run_qaoa(unsigned n, const CostT* cost, unsigned p, const double* gamma, con
         const QaoaPlan pl = qaoa_plan(n, P.C, P.kind, p, P.pass);
         std::vector<double2> vb(size_t(1) << P.C);
         std::vector<double> red(nthr + 32);
-        std::vector<CostT> cb(size_t(1) << P.C);
-        const QaoaSmem<CostT> S{vb.data(), red.data(), cb.data()};
+        const QaoaSmem S{vb.data(), red.data()};
         for (idx_t w = 0; w < P.items; ++w)
             for (unsigned st = 0; st < qaoa_stages(pl); ++st)
                 for (unsigned t = 0; t < nthr; ++t) qaoa_stage<CostT>(P, T, I, pl, mem, cmem, w, st, S, t, nthr);

@@ -148,7 +148,7 @@ def test_tune_and_cache(ork, tmp_path):
         bt.tune(g, b, path)
         for n in ns:
             C, t = bt.config(n)
-            assert t in (256, 512) and C <= 13 and (C >= n or 2 * C >= n)
+            assert t in (128, 256, 512) and C <= 13 and (C >= n or 2 * C >= n)
         after = bt.run(g, b)
         assert np.abs(after - before).max() < TOL
         lines = open(path).read().strip().splitlines()

@@ -96,3 +96,16 @@ def test_regular_maxcut_is_integer_and_bounded():
     g, b = angles(4, 9)
     res, m = kemu.qaoa(n, cost, 4, g, b, log_chunk=7, nthr=64, byte_cost=True)
     assert res.oob == 0 and abs(m - R.qaoa_mean(n, cost, g, b)) < 1e-12
+
+
+@pytest.mark.parametrize("n,C", [(6, 6), (11, 6)])
+def test_mixer_forms_and_edge_angles(n, C):
+    """beta = 0, pi/4 (|cos| = |sin|), pi/2 (cos = 0), and angles outside [0, pi/2] use both
+    four-FMA forms of the rx update; gamma = 0 is the identity phase."""
+    edges, _ = graph(n, 4)
+    cost = R.maxcut_cost(n, edges)
+    g = np.array([0.0, 0.7, np.pi, 2.5, -0.4])
+    b = np.array([0.0, np.pi / 4, np.pi / 2, 3.0, -1.2])
+    res, m = kemu.qaoa(n, cost, 5, g, b, log_chunk=C, nthr=32, byte_cost=True)
+    assert res.oob == 0
+    assert abs(m - R.qaoa_mean(n, cost, g, b)) < 1e-12
