@@ -1,0 +1,241 @@
+"""Binding of the FP32 surrogate network (include/orkan_mlp.h) and the surrogate-guided
+angle search built on it and on the batched simulator (include/orkan_batch.h).
+
+    net = Mlp(ork, n_in=12, hidden=256, max_batch=1024, seed=1)
+    net.train(x_dev, t_dev, epochs=..., batch=1024, lr=1e-3)     # device tensors (torch)
+    y = net.forward(x_dev)
+    x_new = net.ascend(x0_dev, steps=200, lr=0.02)                 # proposals
+
+Device memory comes from torch tensors (plumbing only: every computation is a call into
+liborkan_b200.so); there is no Python fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import OrkanError
+
+
+def _declare(lib):
+    if getattr(lib, "_mlp_declared", False):
+        return
+    P = C.c_void_p
+    lib.orkan_mlp_create.argtypes = [C.POINTER(P), C.c_uint, C.c_uint, C.c_uint, C.c_ulonglong]
+    lib.orkan_mlp_destroy.argtypes = [P]
+    lib.orkan_mlp_destroy.restype = None
+    lib.orkan_mlp_param_count.argtypes = [P]
+    lib.orkan_mlp_param_count.restype = C.c_size_t
+    lib.orkan_mlp_get_params.argtypes = [P, P]
+    lib.orkan_mlp_set_params.argtypes = [P, P]
+    lib.orkan_mlp_forward.argtypes = [P, P, C.c_uint, P, P]
+    lib.orkan_mlp_gradients.argtypes = [P, P, P, C.c_uint, P, P, P, P]
+    lib.orkan_mlp_train.argtypes = [P, P, P, C.c_uint, C.c_uint, C.c_uint, C.c_float, C.c_ulonglong, P, P]
+    lib.orkan_mlp_ascend.argtypes = [P, P, C.c_uint, C.c_uint, C.c_float, C.c_float, C.c_float, P, P]
+    lib.orkan_mlp_launch_count.argtypes = []
+    lib.orkan_mlp_launch_count.restype = C.c_ulonglong
+    for f in ("create", "get_params", "set_params", "forward", "gradients", "train", "ascend"):
+        getattr(lib, "orkan_mlp_" + f).restype = C.c_int
+    lib._mlp_declared = True
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise OrkanError(f"orkan_mlp_{what} failed with CUDA error {rc}")
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream():
+    import torch
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class Mlp:
+    """12 -> hidden -> hidden -> 1 GELU network with its own CUDA kernels."""
+
+    def __init__(self, ork, n_in=12, hidden=256, max_batch=1024, seed=1):
+        self.lib = ork.lib
+        _declare(self.lib)
+        self.n_in, self.hidden, self.max_batch = n_in, hidden, max_batch
+        h = C.c_void_p()
+        _check(self.lib.orkan_mlp_create(C.byref(h), n_in, hidden, max_batch, seed), "create")
+        self.h = h
+
+    @property
+    def param_count(self) -> int:
+        return int(self.lib.orkan_mlp_param_count(self.h))
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.param_count, dtype=np.float32)
+        _check(self.lib.orkan_mlp_get_params(self.h, out.ctypes.data), "get_params")
+        return out
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.param_count
+        _check(self.lib.orkan_mlp_set_params(self.h, p.ctypes.data), "set_params")
+
+    def forward(self, x):
+        import torch
+        n = x.shape[0]
+        y = torch.empty(n, dtype=torch.float32, device=x.device)
+        for c0 in range(0, n, self.max_batch):
+            c1 = min(n, c0 + self.max_batch)
+            xs, ys = x[c0:c1], y[c0:c1]
+            _check(self.lib.orkan_mlp_forward(self.h, _ptr(xs), c1 - c0, _ptr(ys), _stream()), "forward")
+        return y
+
+    def gradients(self, x, t, want_x=False):
+        import torch
+        g = torch.empty(self.param_count, dtype=torch.float32, device=x.device)
+        gx = torch.empty_like(x) if want_x else None
+        loss = torch.empty(1, dtype=torch.float32, device=x.device)
+        _check(self.lib.orkan_mlp_gradients(self.h, _ptr(x), _ptr(t), x.shape[0], _ptr(loss), _ptr(g),
+                                            None if gx is None else _ptr(gx), _stream()), "gradients")
+        return float(loss.item()), g, gx
+
+    def train(self, x, t, epochs, batch=1024, lr=1e-3, seed=0) -> float:
+        import torch
+        loss = torch.empty(1, dtype=torch.float32, device=x.device)
+        _check(self.lib.orkan_mlp_train(self.h, _ptr(x), _ptr(t), x.shape[0], epochs, batch, lr, seed, _ptr(loss),
+                                        _stream()), "train")
+        return float(loss.item())
+
+    def ascend(self, x, steps=200, lr=0.02, lo=-1.0, hi=1.0):
+        """Adam ascent of the network's output over its inputs (in place); returns f(x)."""
+        import torch
+        y = torch.empty(x.shape[0], dtype=torch.float32, device=x.device)
+        _check(self.lib.orkan_mlp_ascend(self.h, _ptr(x), x.shape[0], steps, lr, lo, hi, _ptr(y), _stream()),
+               "ascend")
+        return y
+
+    def close(self):
+        if self.h:
+            self.lib.orkan_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------------------
+# angle encoding: gamma in [0, pi], beta in [0, pi/2]  <->  inputs in [-1, 1]
+# ---------------------------------------------------------------------------------------
+def encode(gammas, betas):
+    g = np.asarray(gammas, dtype=np.float64) / np.pi * 2.0 - 1.0
+    b = np.asarray(betas, dtype=np.float64) / (np.pi / 2.0) * 2.0 - 1.0
+    return np.concatenate([g, b], axis=1).astype(np.float32)
+
+
+def decode(x, p):
+    x = np.asarray(x, dtype=np.float64)
+    return (x[:, :p] + 1.0) / 2.0 * np.pi, (x[:, p:] + 1.0) / 2.0 * (np.pi / 2.0)
+
+
+class Evaluator:
+    """Exact FP64 expectation values of one cost function at many angle sets: a batch of
+    `width` instances of the same graph (one shared cost vector) replayed per call."""
+
+    def __init__(self, ork, n, edges, weights, p, width, density=None):
+        from .batch import QaoaBatch
+        self.p, self.width = p, width
+        self.batch = QaoaBatch(ork, [n] * width, [edges] * width, None if weights is None else [weights] * width, p)
+        self.evals = 0
+
+    def __call__(self, gammas, betas):
+        gammas, betas = np.asarray(gammas), np.asarray(betas)
+        out = np.empty(len(gammas))
+        for c0 in range(0, len(gammas), self.width):
+            c1 = min(len(gammas), c0 + self.width)
+            g = np.zeros((self.width, self.p))
+            b = np.zeros((self.width, self.p))
+            g[:c1 - c0], b[:c1 - c0] = gammas[c0:c1], betas[c0:c1]
+            out[c0:c1] = self.batch.run(g, b)[:c1 - c0]
+            self.evals += c1 - c0
+        return out
+
+    def close(self):
+        self.batch.close()
+
+
+def plain_sweep(evaluate, p, count, rng, chunk, clock):
+    """The method without the network: uniformly random angles in batches; returns the
+    samples, their exact values and the best-so-far trace [(seconds, best)]."""
+    gs, bs, es, trace = [], [], [], []
+    best = -np.inf
+    for c0 in range(0, count, chunk):
+        c = min(chunk, count - c0)
+        g = rng.uniform(0, np.pi, (c, p))
+        b = rng.uniform(0, np.pi / 2, (c, p))
+        e = evaluate(g, b)
+        gs.append(g); bs.append(b); es.append(e)
+        best = max(best, float(e.max()))
+        trace.append((clock(), best))
+    return np.concatenate(gs), np.concatenate(bs), np.concatenate(es), trace
+
+
+def surrogate_search(ork, evaluate, p, g, b, e, target, clock, rng, hidden=256, batch=1024, epochs=60,
+                     rounds=8, proposals=1024, ascent_steps=300, seed=1, log=None):
+    """Train the network on (angles, exact value) pairs, then repeat: propose `proposals`
+    angle sets by Adam ascent on the network from the best known points and random starts,
+    re-score them exactly, add them to the training set and fine-tune; stop once an exactly
+    scored proposal reaches `target`.  Returns (best exact value, seconds, trace, stats)."""
+    import torch
+    dev = torch.device("cuda")
+    x = encode(g, b)
+    mu, sd = float(np.mean(e)), float(np.std(e)) or 1.0
+    net = Mlp(ork, n_in=2 * p, hidden=hidden, max_batch=batch, seed=seed)
+    xs = torch.from_numpy(x).to(dev)
+    ts = torch.from_numpy(((e - mu) / sd).astype(np.float32)).to(dev)
+    stats = {"train_samples": len(e), "epochs": epochs}
+    t0 = clock()
+    loss = net.train(xs, ts, epochs=epochs, batch=batch, lr=1e-3, seed=seed)
+    stats["train_seconds"] = clock() - t0
+    stats["train_loss"] = loss
+    # surrogate error on held-out exact points (fresh uniform samples are not needed: the
+    # proposals below are exactly scored, and their prediction error is recorded per round)
+    best = float(np.max(e))
+    trace = [(clock(), best)]
+    all_x, all_e = x, e
+    errs = []
+    for r in range(rounds):
+        order = np.argsort(-all_e)
+        n_top = proposals // 2
+        starts = all_x[order[:n_top]] + rng.normal(0, 0.05, (n_top, 2 * p)).astype(np.float32)
+        starts = np.concatenate([starts, rng.uniform(-1, 1, (proposals - n_top, 2 * p)).astype(np.float32)])
+        xp = torch.from_numpy(np.clip(starts, -1, 1).astype(np.float32)).to(dev)
+        pred = net.ascend(xp, steps=ascent_steps, lr=0.02)
+        xq = xp.cpu().numpy()
+        gq, bq = decode(xq, p)
+        eq = evaluate(gq, bq)
+        pq = pred.cpu().numpy().astype(np.float64) * sd + mu
+        errs.append(float(np.mean(np.abs(pq - eq))))
+        best = max(best, float(eq.max()))
+        trace.append((clock(), best))
+        if log:
+            log(f"round {r}: best exact {best:.6f}, proposals max {eq.max():.6f}, |pred - exact| mean {errs[-1]:.4f}")
+        all_x = np.concatenate([all_x, xq])
+        all_e = np.concatenate([all_e, eq])
+        if best >= target:
+            break
+        xs = torch.from_numpy(all_x).to(dev)
+        ts = torch.from_numpy(((all_e - mu) / sd).astype(np.float32)).to(dev)
+        net.train(xs, ts, epochs=max(2, epochs // 6), batch=batch, lr=3e-4, seed=seed + r + 1)
+    stats["proposal_abs_err"] = errs
+    stats["rounds"] = len(errs)
+    net.close()
+    return best, trace, stats
+
+
+def now():
+    import torch
+    torch.cuda.synchronize()
+    return time.perf_counter()

@@ -1,0 +1,145 @@
+"""The FP32 surrogate network's CUDA kernels against the CPU oracle (oracle/mlp.py), and the
+surrogate-guided search against the plain batched sweep on a small QAOA instance."""
+import numpy as np
+import pytest
+
+import orkan_b200
+from oracle import mlp as M
+from oracle import restate as R
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ork():
+    return orkan_b200.load(5)
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    return t
+
+
+def rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+
+
+def test_initial_parameters_match_oracle(ork):
+    from orkan_b200.surrogate import Mlp
+    net = Mlp(ork, 12, 256, 1024, seed=5)
+    assert np.array_equal(net.get_params(), M.init_params(12, 256, 5))
+    net.close()
+
+
+@pytest.mark.parametrize("n_in,h,batch", [(12, 256, 1024), (12, 256, 1000), (5, 37, 77)])
+def test_forward_and_gradients_vs_oracle(ork, torch, n_in, h, batch):
+    from orkan_b200.surrogate import Mlp
+    rng = np.random.default_rng(n_in + h + batch)
+    net = Mlp(ork, n_in, h, max(batch, 64), seed=3)
+    p = (rng.normal(0, 1, net.param_count) / np.sqrt(h)).astype(np.float32)
+    net.set_params(p)
+    x = rng.uniform(-1, 1, (batch, n_in)).astype(np.float32)
+    t = rng.normal(0, 1, batch).astype(np.float32)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    y = net.forward(xd).cpu().numpy()
+    y_ref, _ = M.forward(p, x, n_in, h)
+    assert rel(y, y_ref) < 1e-5
+    loss, g, gx = net.gradients(xd, td, want_x=True)
+    loss_ref, g_ref, gx_ref = M.gradients(p, x, t, n_in, h)
+    assert abs(loss - loss_ref) < 1e-5 * max(1.0, loss_ref)
+    g = g.cpu().numpy()
+    # every parameter block separately (FP32 kernels vs float64 oracle)
+    o = 0
+    for size in (n_in * h, h, h * h, h, h, 1):
+        assert rel(g[o:o + size], g_ref[o:o + size]) < 1e-4, f"block at {o}"
+        o += size
+    assert rel(gx.cpu().numpy(), gx_ref) < 1e-4
+    net.close()
+
+
+def test_one_training_step_is_adam_on_the_full_batch_gradient(ork, torch):
+    from orkan_b200.surrogate import Mlp
+    n_in, h, batch = 12, 64, 256
+    rng = np.random.default_rng(8)
+    net = Mlp(ork, n_in, h, batch, seed=2)
+    p0 = net.get_params()
+    x = rng.uniform(-1, 1, (batch, n_in)).astype(np.float32)
+    t = rng.normal(0, 1, batch).astype(np.float32)
+    net.train(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda(), epochs=1, batch=batch, lr=1e-3)
+    _, g, _ = M.gradients(p0, x, t, n_in, h)
+    p1, _, _ = M.adam_step(p0.astype(np.float64), g, np.zeros_like(g), np.zeros_like(g), 1, 1e-3)
+    got = net.get_params()
+    # the first Adam step moves each parameter by lr g / (|g| + 1e-8): compare the moves where
+    # the gradient is well above FP32 rounding, bound them everywhere
+    mv, mv_ref = got.astype(np.float64) - p0, p1 - p0
+    mask = np.abs(g) > 1e-4 * np.abs(g).max()
+    assert mask.mean() > 0.9
+    assert rel(mv[mask], mv_ref[mask]) < 1e-3
+    assert np.abs(mv).max() <= 1e-3 * 1.001
+    net.close()
+
+
+def test_training_fits_a_smooth_function_and_is_deterministic(ork, torch):
+    from orkan_b200.surrogate import Mlp
+    rng = np.random.default_rng(4)
+    x = rng.uniform(-1, 1, (8192, 12)).astype(np.float32)
+    t = (np.sin(2 * x[:, 0]) * np.cos(x[:, 5]) + 0.5 * x[:, 3] * x[:, 7]).astype(np.float32)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    runs = []
+    for _ in range(2):
+        net = Mlp(ork, 12, 256, 1024, seed=9)
+        y0 = net.forward(xd).cpu().numpy()
+        loss = net.train(xd, td, epochs=40, batch=1024, lr=2e-3, seed=1)
+        y1 = net.forward(xd).cpu().numpy()
+        runs.append(net.get_params())
+        net.close()
+        assert np.mean((y1 - t) ** 2) < 0.05 * np.mean((y0 - t) ** 2)
+        assert loss < 0.01
+    assert np.array_equal(runs[0], runs[1])
+
+
+def test_ascent_increases_the_prediction(ork, torch):
+    from orkan_b200.surrogate import Mlp
+    rng = np.random.default_rng(6)
+    x = rng.uniform(-1, 1, (16384, 12)).astype(np.float32)
+    t = (-(x ** 2).sum(axis=1) + x[:, 0]).astype(np.float32)           # maximum at x0 = 0.5, others 0
+    net = Mlp(ork, 12, 256, 1024, seed=1)
+    net.train(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda(), epochs=60, batch=1024, lr=2e-3)
+    x0 = torch.from_numpy(rng.uniform(-1, 1, (300, 12)).astype(np.float32)).cuda()
+    y0 = net.forward(x0).cpu().numpy()
+    y1 = net.ascend(x0, steps=300, lr=0.02).cpu().numpy()
+    xs = x0.cpu().numpy()
+    assert np.all(np.abs(xs) <= 1.0)
+    assert np.mean(y1) > np.mean(y0) + 1.0
+    assert np.abs(xs[:, 0] - 0.5).mean() < 0.25 and np.abs(xs[:, 1:]).mean() < 0.25
+    net.close()
+
+
+def test_surrogate_search_beats_plain_sweep_at_equal_exact_budget(ork):
+    """The network's gain over the method without it: with the same number of exact
+    evaluations, the surrogate-guided search (half the budget as training data from the
+    sweep, half as re-scored proposals) finds a higher exact <C> than the plain sweep."""
+    from orkan_b200.batch import erdos_renyi_graph
+    from orkan_b200.surrogate import Evaluator, now, plain_sweep, surrogate_search
+    rng = np.random.default_rng(21)
+    n, p = 12, 3
+    edges = erdos_renyi_graph(n, 0.3, rng)
+    w = rng.uniform(0, 1, len(edges))
+    ev = Evaluator(ork, n, edges, w, p, width=1024)
+    budget = 8192
+    g, b, e, _ = plain_sweep(ev, p, budget, np.random.default_rng(1), 1024, now)
+    plain_best = float(e.max())
+    half = budget // 2
+    best, trace, stats = surrogate_search(ork, ev, p, g[:half], b[:half], e[:half], target=np.inf, clock=now,
+                                          rng=np.random.default_rng(2), epochs=60, rounds=4, proposals=1024,
+                                          ascent_steps=200)
+    used = half + 1024 * stats["rounds"]
+    assert used <= budget
+    assert best > plain_best + 1e-3, (best, plain_best)
+    # the proposals' exact values are the FP64 simulator's: spot-check one against the oracle
+    cost = R.maxcut_cost(n, edges, w)
+    gg, bb = rng.uniform(0, np.pi, (1, p)), rng.uniform(0, np.pi / 2, (1, p))
+    assert abs(ev(gg, bb)[0] - R.qaoa_mean(n, cost, gg[0], bb[0])) < 1e-12
+    ev.close()
