@@ -19,12 +19,6 @@ using namespace orkan;
 
 namespace {
 
-template <class CostT>
-struct DevCost {
-    const CostT* p;
-    __device__ __forceinline__ CostT ld(idx_t i) const { return __ldg(p + i); }
-};
-
 // cost[x] = sum_e w_e [bit u_e of x != bit v_e of x], edges in the given order.
 template <class CostT>
 __global__ void k_qaoa_cost(CostT* cost, unsigned n, const unsigned char* edges, const double* w, unsigned ne) {
@@ -51,23 +45,51 @@ __global__ void k_qaoa_tables(const unsigned* cmax, const double* gamma, unsigne
     }
 }
 
-template <unsigned NT, class CostT>
-__global__ void __launch_bounds__(NT, NT == 128 ? 3 : 512 / NT) k_qaoa_pass(QaoaPass P, QaoaTables T) {
-    extern __shared__ double2 smem_q[];
-    QaoaSmem S;
-    S.vb = smem_q;
-    S.red = reinterpret_cast<double*>(smem_q + (1u << P.C));
-    for (idx_t w = blockIdx.x; w < P.items; w += gridDim.x) {
+// Persistent pass kernel: each block walks the work items w = blockIdx.x, + gridDim.x, ...
+// With RING = 2 the next item's amplitudes and costs are copied asynchronously into the
+// second shared buffer while the current item is computed; with RING = 1 (2^13-amplitude
+// chunks, which leave no room for a second buffer) the copy follows the item.
+template <unsigned NT, class CostT, unsigned RING>
+__global__ void __launch_bounds__(NT, 1) k_qaoa_pass(QaoaPass P, QaoaTables T) {
+    extern __shared__ __align__(16) unsigned char smem_q[];
+    const unsigned lc = P.kind == kQaoaFull ? P.inst[0].n : P.C;
+    auto fill = [&](idx_t w, unsigned slot) {
         const QaoaInst I = P.inst[qaoa_find(P.inst, P.ninst, w)];
         const QaoaPlan pl = qaoa_plan(I.n, P.C, P.kind, P.p, P.pass);
+        const QaoaSmem<CostT> S = qaoa_smem_at<CostT>(smem_q, lc, NT, RING, slot);
+        qaoa_fill<CostT>(P, I, pl, QaoaDevPsi{I.psi}, QaoaDevCost<CostT>{static_cast<const CostT*>(I.cost)},
+                         w - I.item0, S, threadIdx.x, NT);
+    };
+    unsigned slot = 0;
+    idx_t w = blockIdx.x;
+    if (w < P.items) fill(w, 0);
+    qaoa_cp_commit();
+    for (; w < P.items; w += gridDim.x) {
+        const idx_t wn = w + gridDim.x;
+        if (RING == 2) {
+            if (wn < P.items) fill(wn, slot ^ 1u);
+            qaoa_cp_commit();
+            qaoa_cp_wait<1>();
+        } else {
+            qaoa_cp_wait<0>();
+        }
+        __syncthreads();
+        const QaoaInst I = P.inst[qaoa_find(P.inst, P.ninst, w)];
+        const QaoaPlan pl = qaoa_plan(I.n, P.C, P.kind, P.p, P.pass);
+        const QaoaSmem<CostT> S = qaoa_smem_at<CostT>(smem_q, lc, NT, RING, slot);
         const unsigned nst = qaoa_stages(pl);
-        const DevMem psi{I.psi};
-        const DevCost<CostT> cost{static_cast<const CostT*>(I.cost)};
         for (unsigned st = 0; st < nst; ++st) {
-            qaoa_stage<CostT>(P, T, I, pl, psi, cost, w - I.item0, st, S, threadIdx.x, NT);
+            qaoa_stage<CostT>(P, T, I, pl, QaoaDevPsi{I.psi}, w - I.item0, st, S, threadIdx.x, NT);
             __syncthreads();
         }
+        if (RING == 2) {
+            slot ^= 1u;
+        } else {
+            if (wn < P.items) fill(wn, 0);
+            qaoa_cp_commit();
+        }
     }
+    qaoa_cp_wait<0>();
 }
 
 // out[pos] = sum of the instance's chunk partials, in chunk order
@@ -86,17 +108,20 @@ int sm_count() {
     return v > 0 ? v : 148;
 }
 
-template <unsigned NT, class CostT>
+// The launch shape of a pass: shared bytes, ring depth, and the blocks (every item gets a
+// block, up to the resident blocks of all SMs).  Called before any graph capture: it sets
+// the kernels' shared-memory attribute.
+template <unsigned NT, class CostT, unsigned RING>
 int pass_grid(size_t smem, idx_t items, unsigned* grid) {
     static bool attr = false;
     if (!attr) {
-        const cudaError_t e =
-            cudaFuncSetAttribute(k_qaoa_pass<NT, CostT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        const cudaError_t e = cudaFuncSetAttribute(k_qaoa_pass<NT, CostT, RING>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         if (e != cudaSuccess) return (int)e;
         attr = true;
     }
     int per = 0;
-    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_qaoa_pass<NT, CostT>, NT, smem);
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_qaoa_pass<NT, CostT, RING>, NT, smem);
     if (e != cudaSuccess) return (int)e;
     if (per < 1) return (int)cudaErrorInvalidConfiguration;
     const idx_t cap = (idx_t)sm_count() * per;
@@ -104,21 +129,33 @@ int pass_grid(size_t smem, idx_t items, unsigned* grid) {
     return 0;
 }
 
-// Blocks of a pass launch: every item gets a block, up to the resident blocks of all SMs.
-// (Called before any graph capture: it sets the kernel's shared-memory attribute.)
+constexpr size_t kSmemLimit = 227 * 1024;
+
 template <class CostT>
-int pass_grid_t(unsigned nt, unsigned C, idx_t items, unsigned* grid) {
-    const size_t smem = qaoa_smem_bytes(C, nt);
-    if (nt == 128) return pass_grid<128, CostT>(smem, items, grid);
-    return nt == 256 ? pass_grid<256, CostT>(smem, items, grid) : pass_grid<512, CostT>(smem, items, grid);
+unsigned ring_for(unsigned lc, unsigned nt) {
+    return qaoa_smem_bytes<CostT>(lc, nt, 2) <= kSmemLimit ? 2u : 1u;
 }
 
 template <class CostT>
-int launch_pass_t(unsigned nt, unsigned grid, const QaoaPass& P, const QaoaTables& T, cudaStream_t st) {
-    const size_t smem = qaoa_smem_bytes(P.C, nt);
-    if (nt == 128) k_qaoa_pass<128, CostT><<<grid, 128, smem, st>>>(P, T);
-    else if (nt == 256) k_qaoa_pass<256, CostT><<<grid, 256, smem, st>>>(P, T);
-    else k_qaoa_pass<512, CostT><<<grid, 512, smem, st>>>(P, T);
+int pass_grid_t(unsigned nt, unsigned lc, idx_t items, unsigned* grid) {
+    const unsigned ring = ring_for<CostT>(lc, nt);
+    const size_t smem = qaoa_smem_bytes<CostT>(lc, nt, ring);
+    if (smem > kSmemLimit) return (int)cudaErrorInvalidConfiguration;
+    if (nt == 256) return ring == 2 ? pass_grid<256, CostT, 2>(smem, items, grid) : pass_grid<256, CostT, 1>(smem, items, grid);
+    return ring == 2 ? pass_grid<512, CostT, 2>(smem, items, grid) : pass_grid<512, CostT, 1>(smem, items, grid);
+}
+
+template <class CostT>
+int launch_pass_t(unsigned nt, unsigned lc, unsigned grid, const QaoaPass& P, const QaoaTables& T, cudaStream_t st) {
+    const unsigned ring = ring_for<CostT>(lc, nt);
+    const size_t smem = qaoa_smem_bytes<CostT>(lc, nt, ring);
+    if (nt == 256) {
+        if (ring == 2) k_qaoa_pass<256, CostT, 2><<<grid, 256, smem, st>>>(P, T);
+        else k_qaoa_pass<256, CostT, 1><<<grid, 256, smem, st>>>(P, T);
+    } else {
+        if (ring == 2) k_qaoa_pass<512, CostT, 2><<<grid, 512, smem, st>>>(P, T);
+        else k_qaoa_pass<512, CostT, 1><<<grid, 512, smem, st>>>(P, T);
+    }
     return (int)cudaGetLastError();
 }
 
@@ -310,7 +347,8 @@ int enqueue_kernels(const orkan_qaoa* b, const Plan& pl, cudaStream_t st) {
             P.pass = L.pass;
             P.C = L.C;
             P.kind = L.kind;
-            rc = L.bytes ? launch_pass_t<uint8_t>(L.nt, L.grid, P, T, st) : launch_pass_t<double>(L.nt, L.grid, P, T, st);
+            rc = L.bytes ? launch_pass_t<uint8_t>(L.nt, L.C, L.grid, P, T, st)
+                         : launch_pass_t<double>(L.nt, L.C, L.grid, P, T, st);
         } else {
             k_qaoa_fold<<<(L.ninst + 127) / 128, 128, 0, st>>>(inst, L.ninst, b->d_partial + L.partial_off, L.items,
                                                                b->d_out);
@@ -405,7 +443,7 @@ int orkan_qaoa_create(orkan_qaoa_t** out, unsigned count, const unsigned* n_qubi
     b->n.assign(n_qubits, n_qubits + count);
     for (unsigned q = 0; q <= 26; ++q) {
         b->cfgC[q] = default_C(q);
-        b->cfgT[q] = 128;
+        b->cfgT[q] = 256;
     }
     // distinct graphs (same qubit count, edges in the same order, same weights)
     std::map<std::vector<unsigned char>, unsigned> seen;
@@ -453,7 +491,8 @@ int orkan_qaoa_create(orkan_qaoa_t** out, unsigned count, const unsigned* n_qubi
         const idx_t dim = idx_t(1) << g.n;
         unsigned char* d_e = nullptr;
         double* d_w = nullptr;
-        if ((rc = (int)cudaMalloc(&g.d_cost, dim * (bytes ? 1 : 8))) || (rc = dalloc(&d_e, g.edges.size())) ||
+        const size_t cbytes = bytes ? ((dim + 15) / 16) * 16 : dim * 8;     // byte costs: whole 4-byte words
+        if ((rc = (int)cudaMalloc(&g.d_cost, cbytes)) || (rc = dalloc(&d_e, g.edges.size())) ||
             (rc = dalloc(&d_w, g.w.size()))) {
             cudaFree(d_e);
             orkan_qaoa_destroy(b);
@@ -568,7 +607,7 @@ int orkan_qaoa_tune(orkan_qaoa_t* b, const double* gammas, const double* betas, 
         unsigned C = 0, t = 0;
         if (at != std::string::npos &&
             sscanf(cached.c_str() + at + key.size() + 2, ": {\"C\": %u, \"threads\": %u", &C, &t) == 2 &&
-            C <= kQaoaMaxC && (C >= nq || 2 * C >= nq) && (t == 128 || t == 256 || t == 512)) {
+            C <= kQaoaMaxC && (C >= nq || 2 * C >= nq) && (t == 256 || t == 512)) {
             b->cfgC[nq] = C;
             b->cfgT[nq] = t;
             continue;
@@ -586,7 +625,7 @@ int orkan_qaoa_tune(orkan_qaoa_t* b, const double* gammas, const double* betas, 
         unsigned bestC = b->cfgC[nq], bestT = b->cfgT[nq];
         const unsigned c_lo = std::min(kQaoaMaxC, std::max(10u, (nq + 1) / 2));
         for (unsigned Cc = c_lo; Cc <= kQaoaMaxC; ++Cc) {
-            for (unsigned tt : {128u, 256u, 512u}) {
+            for (unsigned tt : {256u, 512u}) {
                 b->cfgC[nq] = Cc;
                 b->cfgT[nq] = tt;
                 Plan pl = make_plan(b, sel);

@@ -133,9 +133,10 @@ ORKAN_HD unsigned qaoa_find(const QaoaInst* inst, unsigned ninst, idx_t w) {
     return lo;
 }
 
-// Shared-memory slot permutation that keeps the register stages free of bank conflicts
-// for every group position (16-byte amplitudes).
+// Shared-memory slot permutations that keep the register stages free of bank conflicts
+// for every group position (16-byte amplitudes; 8-byte and 4-byte cost words).
 ORKAN_HD unsigned qaoa_sw16(unsigned s) { return s ^ ((s >> 4) & 7u); }
+ORKAN_HD unsigned qaoa_sw8(unsigned s) { return s ^ ((s >> 4) & 15u); }
 
 // What one pass does.
 struct QaoaPlan {
@@ -213,7 +214,7 @@ ORKAN_HD QaoaStage qaoa_reg_stage(const QaoaPlan& pl, unsigned r) {
         s.t1 = (i == pl.m - 1 && t + 1 < pl.segs) ? t + 1 : t;
         s.end0 = i == pl.m - 1;
     }
-    s.src = r == 0 ? (pl.init ? kQaoaFromInit : kQaoaFromGlobal) : kQaoaFromSmem;
+    s.src = (r == 0 && pl.init) ? kQaoaFromInit : kQaoaFromSmem;
     s.dst = r + 1 == pl.nreg ? (pl.measure ? kQaoaToMeasure : kQaoaToGlobal) : kQaoaToSmem;
     s.pre_phase = (r == 0) ? pl.phase_load : -1;
     return s;
@@ -236,14 +237,65 @@ ORKAN_HD double2 qaoa_phase(CostT c, double gamma, const double2* table) {
     }
 }
 
-// Shared memory of one block: vb[2^C] amplitudes, red[nthr + 32] doubles.
+// Shared memory of one block: kQaoaRing buffers, each vb[2^C] amplitudes and cw[2^C] cost
+// words (the 4-byte word holding a byte cost, or the FP64 cost), then red[nthr + 32].
+constexpr unsigned kQaoaRing = 2;
+
+template <class CostT>
+struct QaoaCostWord { typedef uint32_t type; };
+template <>
+struct QaoaCostWord<double> { typedef double type; };
+
+template <class CostT>
 struct QaoaSmem {
     double2* vb;
+    typename QaoaCostWord<CostT>::type* cw;
     double* red;
 };
 
-ORKAN_HD size_t qaoa_smem_bytes(unsigned C, unsigned nthr) {
-    return size_t(16) * (size_t(1) << C) + size_t(8) * (nthr + 32);
+template <class CostT>
+ORKAN_HD size_t qaoa_buffer_bytes(unsigned C) {
+    return (size_t(16) + sizeof(typename QaoaCostWord<CostT>::type)) * (size_t(1) << C);
+}
+template <class CostT>
+ORKAN_HD size_t qaoa_smem_bytes(unsigned C, unsigned nthr, unsigned ring) {
+    return qaoa_buffer_bytes<CostT>(C) * ring + size_t(8) * (nthr + 32);
+}
+template <class CostT>
+ORKAN_HD QaoaSmem<CostT> qaoa_smem_at(unsigned char* base, unsigned C, unsigned nthr, unsigned ring, unsigned slot) {
+    QaoaSmem<CostT> S;
+    unsigned char* b = base + qaoa_buffer_bytes<CostT>(C) * slot;
+    S.vb = reinterpret_cast<double2*>(b);
+    S.cw = reinterpret_cast<typename QaoaCostWord<CostT>::type*>(b + size_t(16) * (size_t(1) << C));
+    S.red = reinterpret_cast<double*>(base + qaoa_buffer_bytes<CostT>(C) * ring);
+    (void)nthr;
+    return S;
+}
+
+// Cost of slot s (global index x) from its staged word.
+template <class CostT>
+ORKAN_HD CostT qaoa_cost_at(const QaoaSmem<CostT>& S, unsigned s, idx_t x) {
+    if constexpr (std::is_same<CostT, double>::value) {
+        (void)x;
+        return S.cw[qaoa_sw8(s)];
+    } else {
+        return (CostT)((S.cw[qaoa_sw8(s)] >> (8u * ((unsigned)x & 3u))) & 0xffu);
+    }
+}
+
+// Fill of one work item's buffer: asynchronous copies of its amplitudes (unless the pass
+// starts from |+>) and cost words, slot s = tid, tid + nthr, ... in order, so consecutive
+// threads copy consecutive amplitudes.  Mem::cp16(dst, x) copies amplitude x,
+// CostMem::cpw(dst, x) the cost word of amplitude x.
+template <class CostT, class Mem, class CostMem>
+ORKAN_HD void qaoa_fill(const QaoaPass& P, const QaoaInst& I, const QaoaPlan& pl, const Mem& psi, const CostMem& cost,
+                        idx_t chunk, const QaoaSmem<CostT>& S, unsigned tid, unsigned nthr) {
+    const unsigned cnt = 1u << qaoa_lc(I.n, P.C, P.kind);
+    for (unsigned s = tid; s < cnt; s += nthr) {
+        const idx_t x = qaoa_index(I.n, P.C, P.kind, chunk, s);
+        if (!pl.init) psi.cp16(S.vb + qaoa_sw16(s), x);
+        cost.cpw(S.cw + qaoa_sw8(s), x);
+    }
 }
 
 ORKAN_HD double qaoa_powu(double x, unsigned e) {
@@ -253,10 +305,10 @@ ORKAN_HD double qaoa_powu(double x, unsigned e) {
 }
 
 // Register stage of a group of K slot bits starting at b0.
-template <int K, class CostT, class Mem, class CostMem>
+template <int K, class CostT, class Mem>
 ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst& I, const QaoaPlan& pl,
-                         const QaoaStage& sg, const Mem& psi, const CostMem& cost, idx_t chunk,
-                         const QaoaSmem& S, unsigned lc, unsigned b0, unsigned tid, unsigned nthr) {
+                         const QaoaStage& sg, const Mem& psi, idx_t chunk, const QaoaSmem<CostT>& S, unsigned lc,
+                         unsigned b0, unsigned tid, unsigned nthr) {
     constexpr unsigned NV = 1u << K;
     const unsigned n = I.n;
     const unsigned sets = 1u << (lc - K);
@@ -266,32 +318,38 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
     const idx_t row = (idx_t)I.pos * P.p;
     const bool need_cost = sg.pre_phase >= 0 || sg.t1 > sg.t0 || sg.dst == kQaoaToMeasure;
     const double amp0 = 1.0 / sqrt((double)(idx_t(1) << n));
+    // shared-memory slot of element j: the swizzles are XOR-linear and base, j << b0 have
+    // disjoint bits, so sw(base | j << b0) = sw(base) ^ sw(j << b0)
+    unsigned o16[NV], o8[NV];
+#pragma unroll
+    for (unsigned j = 0; j < NV; ++j) {
+        o16[j] = qaoa_sw16(j << b0);
+        o8[j] = qaoa_sw8(j << b0);
+    }
     double acc = 0.0;
     for (unsigned r = tid; r < sets; r += nthr) {
         const unsigned base = (r & lowm) | ((r >> b0) << (b0 + K));
+        const unsigned sb16 = qaoa_sw16(base), sb8 = qaoa_sw8(base);
         const idx_t xb = qaoa_index(n, P.C, P.kind, chunk, base);      // slot base | j << b0 is xb + j xs
         double2 v[NV];
         CostT cv[NV];
-        if (sg.src == kQaoaFromGlobal) {
+        if (sg.src == kQaoaFromSmem) {
 #pragma unroll
-            for (unsigned j = 0; j < NV; ++j) v[j] = psi.ld(xb + j * xs);
-        } else if (sg.src == kQaoaFromSmem) {
-#pragma unroll
-            for (unsigned j = 0; j < NV; ++j) v[j] = S.vb[qaoa_sw16(base | (j << b0))];
+            for (unsigned j = 0; j < NV; ++j) v[j] = S.vb[sb16 ^ o16[j]];
         } else {
 #pragma unroll
             for (unsigned j = 0; j < NV; ++j) v[j] = c2(amp0, 0.0);
         }
-        // byte costs are fetched with the amplitudes; FP64 costs (twice the registers) when
-        // first needed
-        bool have_cost = false;
-        auto fetch_cost = [&]() {
-            if (have_cost) return;
+        if (need_cost) {
+            if constexpr (std::is_same<CostT, double>::value) {
 #pragma unroll
-            for (unsigned j = 0; j < NV; ++j) cv[j] = cost.ld(xb + j * xs);
-            have_cost = true;
-        };
-        if (need_cost && (sizeof(CostT) == 1 || sg.pre_phase >= 0)) fetch_cost();
+                for (unsigned j = 0; j < NV; ++j) cv[j] = S.cw[sb8 ^ o8[j]];
+            } else {
+#pragma unroll
+                for (unsigned j = 0; j < NV; ++j)
+                    cv[j] = (CostT)((S.cw[sb8 ^ o8[j]] >> (8u * ((unsigned)(xb + j * xs) & 3u))) & 0xffu);
+            }
+        }
         if (sg.pre_phase >= 0) {
             const unsigned layer = pl.layer0 + (unsigned)sg.pre_phase;
             const double gam = P.gamma[row + layer];
@@ -330,7 +388,6 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
             }
             const bool ends = (pl.m == 1) || (t == sg.t0 && sg.end0);
             if (t < sg.t1) {                                  // scale of segment t, phase of the next layer
-                fetch_cost();
                 const double f = qaoa_powu(rx.scale, nq);
                 const double gam = P.gamma[row + layer + 1];
                 const double2* tb = T.phase + (row + layer + 1) * T.tstride;
@@ -346,7 +403,6 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
             }
         }
         if (sg.dst == kQaoaToMeasure) {
-            fetch_cost();
 #pragma unroll
             for (unsigned j = 0; j < NV; ++j) acc += (double)cv[j] * (v[j].x * v[j].x + v[j].y * v[j].y);
         } else if (sg.dst == kQaoaToGlobal) {
@@ -354,18 +410,18 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
             for (unsigned j = 0; j < NV; ++j) psi.st(xb + j * xs, v[j]);
         } else {
 #pragma unroll
-            for (unsigned j = 0; j < NV; ++j) S.vb[qaoa_sw16(base | (j << b0))] = v[j];
+            for (unsigned j = 0; j < NV; ++j) S.vb[sb16 ^ o16[j]] = v[j];
         }
     }
     if (sg.dst == kQaoaToMeasure) S.red[tid] = acc;
 }
 
-// Per-thread work of stage `st` of one work item (instance I, chunk index `chunk`).
-// Barriers between the stages are the caller's.
-template <class CostT, class Mem, class CostMem>
+// Per-thread work of stage `st` of one work item (instance I, chunk index `chunk`) whose
+// buffer S was filled by qaoa_fill.  Barriers between the stages are the caller's.
+template <class CostT, class Mem>
 ORKAN_HD void qaoa_stage(const QaoaPass& P, const QaoaTables& T, const QaoaInst& I, const QaoaPlan& pl,
-                         const Mem& psi, const CostMem& cost, idx_t chunk, unsigned st, const QaoaSmem& S,
-                         unsigned tid, unsigned nthr) {
+                         const Mem& psi, idx_t chunk, unsigned st, const QaoaSmem<CostT>& S, unsigned tid,
+                         unsigned nthr) {
     const unsigned n = I.n, kind = P.kind;
     if (st < pl.nreg) {
         const QaoaStage sg = qaoa_reg_stage(pl, st);
@@ -375,10 +431,10 @@ ORKAN_HD void qaoa_stage(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
         const unsigned k = (nq - off) < kQaoaGroup ? nq - off : kQaoaGroup;
         const unsigned b0 = qaoa_bit(n, P.C, kind, pl.q0 + off);
         switch (k) {
-            case 1: qaoa_group<1, CostT>(P, T, I, pl, sg, psi, cost, chunk, S, lc, b0, tid, nthr); break;
-            case 2: qaoa_group<2, CostT>(P, T, I, pl, sg, psi, cost, chunk, S, lc, b0, tid, nthr); break;
-            case 3: qaoa_group<3, CostT>(P, T, I, pl, sg, psi, cost, chunk, S, lc, b0, tid, nthr); break;
-            default: qaoa_group<4, CostT>(P, T, I, pl, sg, psi, cost, chunk, S, lc, b0, tid, nthr); break;
+            case 1: qaoa_group<1, CostT>(P, T, I, pl, sg, psi, chunk, S, lc, b0, tid, nthr); break;
+            case 2: qaoa_group<2, CostT>(P, T, I, pl, sg, psi, chunk, S, lc, b0, tid, nthr); break;
+            case 3: qaoa_group<3, CostT>(P, T, I, pl, sg, psi, chunk, S, lc, b0, tid, nthr); break;
+            default: qaoa_group<4, CostT>(P, T, I, pl, sg, psi, chunk, S, lc, b0, tid, nthr); break;
         }
         return;
     }
@@ -395,5 +451,38 @@ ORKAN_HD void qaoa_stage(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
         P.partial[I.item0 + chunk] = s;
     }
 }
+
+#ifdef __CUDACC__
+// Device accessors: amplitude loads/stores and the asynchronous 16-byte copy of the fill.
+struct QaoaDevPsi {
+    double2* p;
+    __device__ __forceinline__ void st(idx_t i, double2 v) const { p[i] = v; }
+    __device__ __forceinline__ void cp16(double2* dst, idx_t i) const {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(p + i) : "memory");
+    }
+};
+template <class CostT>
+struct QaoaDevCost;
+template <>
+struct QaoaDevCost<double> {
+    const double* p;
+    __device__ __forceinline__ void cpw(double* dst, idx_t i) const {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(p + i) : "memory");
+    }
+};
+template <>
+struct QaoaDevCost<uint8_t> {
+    const uint8_t* p;            // allocated in whole 16-byte units
+    __device__ __forceinline__ void cpw(uint32_t* dst, idx_t i) const {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(p + (i & ~idx_t(3))) : "memory");
+    }
+};
+__device__ __forceinline__ void qaoa_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void qaoa_cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+#endif
 
 }  // namespace orkan

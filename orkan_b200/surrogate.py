@@ -144,10 +144,13 @@ class Evaluator:
     """Exact FP64 expectation values of one cost function at many angle sets: a batch of
     `width` instances of the same graph (one shared cost vector) replayed per call."""
 
-    def __init__(self, ork, n, edges, weights, p, width, density=None):
+    def __init__(self, ork, n, edges, weights, p, width, tune=True, cache_path=None):
         from .batch import QaoaBatch
         self.p, self.width = p, width
         self.batch = QaoaBatch(ork, [n] * width, [edges] * width, None if weights is None else [weights] * width, p)
+        if tune:
+            rng = np.random.default_rng(0)
+            self.batch.tune(rng.uniform(0, np.pi, (width, p)), rng.uniform(0, np.pi / 2, (width, p)), cache_path)
         self.evals = 0
 
     def __call__(self, gammas, betas):

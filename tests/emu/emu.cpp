@@ -48,6 +48,11 @@ struct EmuMem {
         *dst = p[i];
     }
     mutable idx_t last_cp = ~idx_t(0);
+    void cp16(double2* dst, idx_t i) const {
+        if (i >= len) { ++*oob; return; }
+        ++reads[i];
+        *dst = p[i];
+    }
     // bulk copies of the GPU path (TMA): n consecutive elements, land immediately here
     void bulk_load(double2* sdst, idx_t i, unsigned n, void*) const {
         for (unsigned k = 0; k < n; ++k) sdst[k] = ld(i + k);
@@ -77,14 +82,23 @@ struct EmuMemC2 {
     }
 };
 
+// Cost vector accessor of the QAOA fill: the FP64 cost of amplitude i, or the 4-byte word
+// holding byte cost i (len counts the allocated bytes, whole 16-byte units).
 template <class CostT>
 struct EmuCost {
     const CostT* p;
     idx_t len;
     uint64_t* oob;
-    CostT ld(idx_t i) const {
-        if (i >= len) { ++*oob; return CostT(0); }
-        return p[i];
+    void cpw(double* dst, idx_t i) const {
+        if (i >= len) { ++*oob; return; }
+        *dst = (double)p[i];
+    }
+    void cpw(uint32_t* dst, idx_t i) const {
+        const idx_t a = i & ~idx_t(3);
+        if (a + 4 > len) { ++*oob; return; }
+        uint32_t w;
+        memcpy(&w, reinterpret_cast<const uint8_t*>(p) + a, 4);
+        *dst = w;
     }
 };
 
@@ -183,7 +197,8 @@ int run_qaoa(unsigned n, const CostT* cost, unsigned p, const double* gamma, con
     I.n = n;
     I.pos = 0;
     const EmuMem mem{reinterpret_cast<double2*>(psi), dim, reads, writes, oob};
-    const EmuCost<CostT> cmem{cost, dim, oob};
+    const idx_t clen = sizeof(CostT) == 1 ? ((dim + 15) / 16) * 16 : dim;
+    const EmuCost<CostT> cmem{cost, clen, oob};
     const unsigned npass = full ? 1 : p + 1;
     for (unsigned j = 0; j < npass && j <= upto; ++j) {
         QaoaPass P;
@@ -199,12 +214,13 @@ int run_qaoa(unsigned n, const CostT* cost, unsigned p, const double* gamma, con
         P.pass = full ? 0 : j;
         const QaoaTables T{table.data(), rx.data(), tstride};
         const QaoaPlan pl = qaoa_plan(n, P.C, P.kind, p, P.pass);
-        std::vector<double2> vb(size_t(1) << P.C);
-        std::vector<double> red(nthr + 32);
-        const QaoaSmem S{vb.data(), red.data()};
-        for (idx_t w = 0; w < P.items; ++w)
+        std::vector<unsigned char> smem(qaoa_smem_bytes<CostT>(P.C, nthr, 1));
+        const QaoaSmem<CostT> S = qaoa_smem_at<CostT>(smem.data(), P.C, nthr, 1, 0);
+        for (idx_t w = 0; w < P.items; ++w) {
+            for (unsigned t = 0; t < nthr; ++t) qaoa_fill<CostT>(P, I, pl, mem, cmem, w, S, t, nthr);
             for (unsigned st = 0; st < qaoa_stages(pl); ++st)
-                for (unsigned t = 0; t < nthr; ++t) qaoa_stage<CostT>(P, T, I, pl, mem, cmem, w, st, S, t, nthr);
+                for (unsigned t = 0; t < nthr; ++t) qaoa_stage<CostT>(P, T, I, pl, mem, w, st, S, t, nthr);
+        }
         if (pl.measure) {
             double s = 0.0;
             for (idx_t w = 0; w < P.items; ++w) s += partial[w];

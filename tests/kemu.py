@@ -179,7 +179,9 @@ def qaoa(n, cost, p, gammas, betas, log_chunk, nthr=64, upto=None, byte_cost=Fal
     """Fused QAOA passes 0..upto of one instance; returns (Result over psi, mean or None)."""
     dim = 1 << n
     cd = _arr(cost, np.float64)
-    cb = _arr(np.asarray(cost), np.uint8) if byte_cost else np.zeros(1, np.uint8)
+    cb = np.zeros(max(16, (dim + 15) // 16 * 16), np.uint8)        # whole 16-byte units, as on the device
+    if byte_cost:
+        cb[:dim] = np.asarray(cost, dtype=np.uint8)
     g = _arr(gammas, np.float64)
     bt = _arr(betas, np.float64)
     mean = C.c_double(float("nan"))
