@@ -47,14 +47,17 @@ int orkan_qaoa_create(orkan_qaoa_t **out, unsigned count, const unsigned *n_qubi
  * means[i] receives the expectation value of the cost.  Synchronises the stream. */
 int orkan_qaoa_run(orkan_qaoa_t *b, const double *gammas, const double *betas, double *means, void *stream);
 
-/* Autotune the chunk size and block size on this batch (timing candidate launch plans on
- * the device with the given angles), keep the fastest and rebuild the graph.  When
+/* Autotune chunk size, block size and buffer depth per qubit count on this batch (timing
+ * candidate launch plans on the device with the given angles), keep the fastest and rebuild
+ * the graph.  When
  * cache_path is not NULL the choice is read from / stored in that JSON file, keyed by the
  * device name and the batch's qubit counts. */
 int orkan_qaoa_tune(orkan_qaoa_t *b, const double *gammas, const double *betas, const char *cache_path);
 
-/* Current launch configuration: log2 chunk for instances of n qubits, threads per block. */
-int orkan_qaoa_config(const orkan_qaoa_t *b, unsigned n, unsigned *log_chunk, unsigned *threads);
+/* Current launch configuration of instances of n qubits: log2 of the chunk (amplitudes per
+ * work item), threads per block, and the number of shared buffers per block (2: the next
+ * item is copied in while the current one computes). */
+int orkan_qaoa_config(const orkan_qaoa_t *b, unsigned n, unsigned *log_chunk, unsigned *threads, unsigned *ring);
 
 /* Copy the device cost vector of instance i (2^n doubles) to host memory (for checks). */
 int orkan_qaoa_cost_vector(orkan_qaoa_t *b, unsigned i, double *host_out);

@@ -23,7 +23,7 @@ def _declare(lib):
     lib.orkan_qaoa_create.argtypes = [C.POINTER(P), C.c_uint, P, P, P, P, C.c_uint, C.c_ulonglong, C.c_uint]
     lib.orkan_qaoa_run.argtypes = [P, P, P, P, P]
     lib.orkan_qaoa_tune.argtypes = [P, P, P, C.c_char_p]
-    lib.orkan_qaoa_config.argtypes = [P, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]
+    lib.orkan_qaoa_config.argtypes = [P, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.POINTER(C.c_uint)]
     lib.orkan_qaoa_cost_vector.argtypes = [P, C.c_uint, P]
     lib.orkan_qaoa_stats.argtypes = [P, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]
     lib.orkan_qaoa_destroy.argtypes = [P]
@@ -82,10 +82,11 @@ class QaoaBatch:
         path = None if cache_path is None else cache_path.encode()
         _check(self.lib.orkan_qaoa_tune(self.h, g.ctypes.data, b.ctypes.data, path), "tune")
 
-    def config(self, n: int) -> tuple[int, int]:
-        lc, t = C.c_uint(), C.c_uint()
-        _check(self.lib.orkan_qaoa_config(self.h, n, C.byref(lc), C.byref(t)), "config")
-        return lc.value, t.value
+    def config(self, n: int) -> tuple[int, int, int]:
+        """(log2 chunk, threads per block, shared buffers per block) for n-qubit instances."""
+        lc, t, r = C.c_uint(), C.c_uint(), C.c_uint()
+        _check(self.lib.orkan_qaoa_config(self.h, n, C.byref(lc), C.byref(t), C.byref(r)), "config")
+        return lc.value, t.value, r.value
 
     def cost_vector(self, i: int) -> np.ndarray:
         out = np.empty(1 << int(self.n[i]), dtype=np.float64)

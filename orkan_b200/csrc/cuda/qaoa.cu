@@ -50,7 +50,7 @@ __global__ void k_qaoa_tables(const unsigned* cmax, const double* gamma, unsigne
 // second shared buffer while the current item is computed; with RING = 1 (2^13-amplitude
 // chunks, which leave no room for a second buffer) the copy follows the item.
 template <unsigned NT, class CostT, unsigned RING>
-__global__ void __launch_bounds__(NT, 1) k_qaoa_pass(QaoaPass P, QaoaTables T) {
+__global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_qaoa_pass(QaoaPass P, QaoaTables T) {
     extern __shared__ __align__(16) unsigned char smem_q[];
     const unsigned lc = P.kind == kQaoaFull ? P.inst[0].n : P.C;
     auto fill = [&](idx_t w, unsigned slot) {
@@ -131,33 +131,40 @@ int pass_grid(size_t smem, idx_t items, unsigned* grid) {
 
 constexpr size_t kSmemLimit = 227 * 1024;
 
-template <class CostT>
-unsigned ring_for(unsigned lc, unsigned nt) {
-    return qaoa_smem_bytes<CostT>(lc, nt, 2) <= kSmemLimit ? 2u : 1u;
+template <unsigned NT, class CostT>
+int pass_grid_n(unsigned ring, size_t smem, idx_t items, unsigned* grid) {
+    return ring == 2 ? pass_grid<NT, CostT, 2>(smem, items, grid) : pass_grid<NT, CostT, 1>(smem, items, grid);
 }
 
 template <class CostT>
-int pass_grid_t(unsigned nt, unsigned lc, idx_t items, unsigned* grid) {
-    const unsigned ring = ring_for<CostT>(lc, nt);
+int pass_grid_t(unsigned nt, unsigned ring, unsigned lc, idx_t items, unsigned* grid) {
     const size_t smem = qaoa_smem_bytes<CostT>(lc, nt, ring);
     if (smem > kSmemLimit) return (int)cudaErrorInvalidConfiguration;
-    if (nt == 256) return ring == 2 ? pass_grid<256, CostT, 2>(smem, items, grid) : pass_grid<256, CostT, 1>(smem, items, grid);
-    return ring == 2 ? pass_grid<512, CostT, 2>(smem, items, grid) : pass_grid<512, CostT, 1>(smem, items, grid);
+    if (nt == 128) return pass_grid_n<128, CostT>(ring, smem, items, grid);
+    if (nt == 256) return pass_grid_n<256, CostT>(ring, smem, items, grid);
+    return pass_grid_n<512, CostT>(ring, smem, items, grid);
+}
+
+template <unsigned NT, class CostT>
+void launch_n(unsigned ring, unsigned grid, size_t smem, const QaoaPass& P, const QaoaTables& T, cudaStream_t st) {
+    if (ring == 2) k_qaoa_pass<NT, CostT, 2><<<grid, NT, smem, st>>>(P, T);
+    else k_qaoa_pass<NT, CostT, 1><<<grid, NT, smem, st>>>(P, T);
 }
 
 template <class CostT>
-int launch_pass_t(unsigned nt, unsigned lc, unsigned grid, const QaoaPass& P, const QaoaTables& T, cudaStream_t st) {
-    const unsigned ring = ring_for<CostT>(lc, nt);
+int launch_pass_t(unsigned nt, unsigned ring, unsigned lc, unsigned grid, const QaoaPass& P, const QaoaTables& T,
+                  cudaStream_t st) {
     const size_t smem = qaoa_smem_bytes<CostT>(lc, nt, ring);
-    if (nt == 256) {
-        if (ring == 2) k_qaoa_pass<256, CostT, 2><<<grid, 256, smem, st>>>(P, T);
-        else k_qaoa_pass<256, CostT, 1><<<grid, 256, smem, st>>>(P, T);
-    } else {
-        if (ring == 2) k_qaoa_pass<512, CostT, 2><<<grid, 512, smem, st>>>(P, T);
-        else k_qaoa_pass<512, CostT, 1><<<grid, 512, smem, st>>>(P, T);
-    }
+    if (nt == 128) launch_n<128, CostT>(ring, grid, smem, P, T, st);
+    else if (nt == 256) launch_n<256, CostT>(ring, grid, smem, P, T, st);
+    else launch_n<512, CostT>(ring, grid, smem, P, T, st);
     return (int)cudaGetLastError();
 }
+
+// Launch configuration of the instances of one qubit count: log2 chunk, threads, ring depth.
+struct QaoaCfg {
+    unsigned C, nt, ring;
+};
 
 struct Graph {                     // one distinct cost function
     unsigned n;
@@ -171,7 +178,7 @@ struct Launch {
     int what;                      // 0 pass, 1 fold
     unsigned inst_off, ninst;      // slice of the plan's instance records
     idx_t items;
-    unsigned pass, C, kind, nt;
+    unsigned pass, C, kind, nt, ring;
     unsigned grid;                 // blocks (pass launches)
     bool bytes;                    // byte costs
     size_t partial_off;
@@ -196,7 +203,7 @@ struct orkan_qaoa {
     unsigned tstride = 1;
     bool any_bytes = false;
     unsigned long long budget = 0;
-    unsigned cfgC[27], cfgT[27];        // launch configuration by qubit count
+    QaoaCfg cfg[27];                    // launch configuration by qubit count
     // device buffers
     unsigned* d_cmax = nullptr;
     double* d_gamma = nullptr;          // [instance][p]
@@ -225,7 +232,17 @@ int dalloc(T** p, size_t count) {
 }
 
 unsigned default_C(unsigned n) { return n <= 12 ? n : std::max(12u, (n + 1) / 2); }
-bool is_full(const orkan_qaoa* b, unsigned n) { return n <= b->cfgC[n]; }
+bool is_full(const orkan_qaoa* b, unsigned n) { return n <= b->cfg[n].C; }
+
+// Default: 2^12-amplitude chunks, 256 threads (one 16-amplitude set per thread and stage),
+// one buffer, so that two blocks share an SM; instances up to 12 qubits in one full pass.
+QaoaCfg default_cfg(unsigned n) {
+    QaoaCfg c;
+    c.C = default_C(n);
+    c.nt = c.C >= 13 ? 512u : c.C >= 12 ? 256u : 128u;
+    c.ring = 1;
+    return c;
+}
 size_t state_bytes(const orkan_qaoa* b, unsigned n) { return is_full(b, n) ? 0 : (size_t(1) << n) * 16; }
 
 // Launch plan for the instances `sel` (qubit counts descending), in waves under the budget.
@@ -254,7 +271,7 @@ Plan make_plan(const orkan_qaoa* b, const std::vector<unsigned>& sel) {
                     if ((b->cmax[sel[k]] < kQaoaMaxTable) == (bool)bytes_cost) grp.push_back(k);
                 if (grp.empty()) continue;
                 const bool full = is_full(b, nq);
-                const unsigned C = full ? nq : b->cfgC[nq];
+                const unsigned C = full ? nq : b->cfg[nq].C;
                 const unsigned npass = full ? 1 : b->p + 1;
                 Launch meas{};
                 for (unsigned j = 0; j < npass; ++j) {
@@ -265,7 +282,8 @@ Plan make_plan(const orkan_qaoa* b, const std::vector<unsigned>& sel) {
                     L.pass = full ? 0 : j;
                     L.C = C;
                     L.kind = full ? kQaoaFull : ((j % 2 == 0) ? kQaoaLow : kQaoaHigh);
-                    L.nt = b->cfgT[nq];
+                    L.nt = b->cfg[nq].nt;
+                    L.ring = b->cfg[nq].ring;
                     L.bytes = bytes_cost;
                     idx_t acc = 0;
                     for (size_t k : grp) {
@@ -316,7 +334,8 @@ int upload_plan(orkan_qaoa* b, Plan& pl) {
     }
     for (auto& L : pl.launches) {
         if (L.what != 0) continue;
-        rc = L.bytes ? pass_grid_t<uint8_t>(L.nt, L.C, L.items, &L.grid) : pass_grid_t<double>(L.nt, L.C, L.items, &L.grid);
+        rc = L.bytes ? pass_grid_t<uint8_t>(L.nt, L.ring, L.C, L.items, &L.grid)
+                     : pass_grid_t<double>(L.nt, L.ring, L.C, L.items, &L.grid);
         if (rc) return rc;
     }
     for (auto& r : pl.inst) r.psi = reinterpret_cast<double2*>(b->d_arena + reinterpret_cast<size_t>(r.psi));
@@ -347,8 +366,8 @@ int enqueue_kernels(const orkan_qaoa* b, const Plan& pl, cudaStream_t st) {
             P.pass = L.pass;
             P.C = L.C;
             P.kind = L.kind;
-            rc = L.bytes ? launch_pass_t<uint8_t>(L.nt, L.C, L.grid, P, T, st)
-                         : launch_pass_t<double>(L.nt, L.C, L.grid, P, T, st);
+            rc = L.bytes ? launch_pass_t<uint8_t>(L.nt, L.ring, L.C, L.grid, P, T, st)
+                         : launch_pass_t<double>(L.nt, L.ring, L.C, L.grid, P, T, st);
         } else {
             k_qaoa_fold<<<(L.ninst + 127) / 128, 128, 0, st>>>(inst, L.ninst, b->d_partial + L.partial_off, L.items,
                                                                b->d_out);
@@ -442,8 +461,7 @@ int orkan_qaoa_create(orkan_qaoa_t** out, unsigned count, const unsigned* n_qubi
     b->p = p;
     b->n.assign(n_qubits, n_qubits + count);
     for (unsigned q = 0; q <= 26; ++q) {
-        b->cfgC[q] = default_C(q);
-        b->cfgT[q] = 256;
+        b->cfg[q] = default_cfg(q);
     }
     // distinct graphs (same qubit count, edges in the same order, same weights)
     std::map<std::vector<unsigned char>, unsigned> seen;
@@ -549,10 +567,11 @@ int orkan_qaoa_run(orkan_qaoa_t* b, const double* gammas, const double* betas, d
     return 0;
 }
 
-int orkan_qaoa_config(const orkan_qaoa_t* b, unsigned n, unsigned* log_chunk, unsigned* threads) {
+int orkan_qaoa_config(const orkan_qaoa_t* b, unsigned n, unsigned* log_chunk, unsigned* threads, unsigned* ring) {
     if (!b || n > 26) return (int)cudaErrorInvalidValue;
-    if (log_chunk) *log_chunk = b->cfgC[n];
-    if (threads) *threads = b->cfgT[n];
+    if (log_chunk) *log_chunk = b->cfg[n].C;
+    if (threads) *threads = b->cfg[n].nt;
+    if (ring) *ring = b->cfg[n].ring;
     return 0;
 }
 
@@ -604,12 +623,13 @@ int orkan_qaoa_tune(orkan_qaoa_t* b, const double* gammas, const double* betas, 
         const unsigned nq = grp.first;
         const std::string key = cache_key(b, nq, grp.second);
         const size_t at = cached.find("\"" + key + "\"");
-        unsigned C = 0, t = 0;
+        QaoaCfg c{};
         if (at != std::string::npos &&
-            sscanf(cached.c_str() + at + key.size() + 2, ": {\"C\": %u, \"threads\": %u", &C, &t) == 2 &&
-            C <= kQaoaMaxC && (C >= nq || 2 * C >= nq) && (t == 256 || t == 512)) {
-            b->cfgC[nq] = C;
-            b->cfgT[nq] = t;
+            sscanf(cached.c_str() + at + key.size() + 2, ": {\"C\": %u, \"threads\": %u, \"ring\": %u", &c.C, &c.nt,
+                   &c.ring) == 3 &&
+            c.C <= kQaoaMaxC && (c.C >= nq || 2 * c.C >= nq) && (c.nt == 128 || c.nt == 256 || c.nt == 512) &&
+            (c.ring == 1 || c.ring == 2)) {
+            b->cfg[nq] = c;
             continue;
         }
         // up to 64 instances of the group, within one wave's budget
@@ -622,31 +642,40 @@ int orkan_qaoa_tune(orkan_qaoa_t* b, const double* gammas, const double* betas, 
                 sel.push_back(i);
             }
         float best = 1e30f;
-        unsigned bestC = b->cfgC[nq], bestT = b->cfgT[nq];
-        const unsigned c_lo = std::min(kQaoaMaxC, std::max(10u, (nq + 1) / 2));
+        QaoaCfg bestc = b->cfg[nq];
+        // chunks from the smallest that keeps the high pass possible (2C >= n) up to 2^13;
+        // a chunk of at least n qubits is the full pass, where only n matters
+        const unsigned c_lo = std::min(kQaoaMaxC, std::max(nq <= 11 ? nq : 11u, (nq + 1) / 2));
         for (unsigned Cc = c_lo; Cc <= kQaoaMaxC; ++Cc) {
-            for (unsigned tt : {256u, 512u}) {
-                b->cfgC[nq] = Cc;
-                b->cfgT[nq] = tt;
-                Plan pl = make_plan(b, sel);
-                if (upload_plan(b, pl)) { cudaGetLastError(); continue; }
-                if (enqueue_kernels(b, pl, b->cap)) { cudaGetLastError(); continue; }   // warm-up
-                cudaEventRecord(e0, b->cap);
-                bool ok = true;
-                for (int r = 0; r < 3 && ok; ++r) ok = enqueue_kernels(b, pl, b->cap) == 0;
-                cudaEventRecord(e1, b->cap);
-                if (!ok || cudaEventSynchronize(e1) != cudaSuccess) { cudaGetLastError(); continue; }
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (ms < best) { best = ms; bestC = Cc; bestT = tt; }
+            const unsigned lc = Cc >= nq ? nq : Cc;
+            for (unsigned tt : {128u, 256u, 512u}) {
+                const unsigned sets = (1u << lc) / 16;       // 16-amplitude sets of a register stage
+                if (tt > std::max(128u, sets) || tt * 4 < sets) continue;
+                for (unsigned rg : {1u, 2u}) {
+                    const bool bytes_cost = grp.second;
+                    const size_t smem = bytes_cost ? qaoa_smem_bytes<uint8_t>(lc, tt, rg) : qaoa_smem_bytes<double>(lc, tt, rg);
+                    if (smem > kSmemLimit) continue;
+                    b->cfg[nq] = QaoaCfg{Cc, tt, rg};
+                    Plan pl = make_plan(b, sel);
+                    if (upload_plan(b, pl)) { cudaGetLastError(); continue; }
+                    if (enqueue_kernels(b, pl, b->cap)) { cudaGetLastError(); continue; }   // warm-up
+                    cudaEventRecord(e0, b->cap);
+                    bool ok = true;
+                    for (int r = 0; r < 3 && ok; ++r) ok = enqueue_kernels(b, pl, b->cap) == 0;
+                    cudaEventRecord(e1, b->cap);
+                    if (!ok || cudaEventSynchronize(e1) != cudaSuccess) { cudaGetLastError(); continue; }
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (ms < best) { best = ms; bestc = b->cfg[nq]; }
+                }
             }
             if (Cc >= nq) break;                            // a full pass: larger chunks change nothing
         }
-        b->cfgC[nq] = bestC;
-        b->cfgT[nq] = bestT;
+        b->cfg[nq] = bestc;
         char line[512];
-        snprintf(line, sizeof line, "{\"%s\": {\"C\": %u, \"threads\": %u, \"ms_per_instance\": %.5f}}\n", key.c_str(),
-                 bestC, bestT, best / 3 / (sel.empty() ? 1 : sel.size()));
+        snprintf(line, sizeof line,
+                 "{\"%s\": {\"C\": %u, \"threads\": %u, \"ring\": %u, \"ms_per_instance\": %.5f}}\n", key.c_str(),
+                 bestc.C, bestc.nt, bestc.ring, best / 3 / (sel.empty() ? 1 : sel.size()));
         append += line;
     }
     cudaEventDestroy(e0);

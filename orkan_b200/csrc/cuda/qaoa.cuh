@@ -316,46 +316,57 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
     const idx_t xs = qaoa_stride(n, P.C, P.kind, b0);
     const unsigned nq = pl.q1 - pl.q0;
     const idx_t row = (idx_t)I.pos * P.p;
-    const bool need_cost = sg.pre_phase >= 0 || sg.t1 > sg.t0 || sg.dst == kQaoaToMeasure;
     const double amp0 = 1.0 / sqrt((double)(idx_t(1) << n));
     // shared-memory slot of element j: the swizzles are XOR-linear and base, j << b0 have
-    // disjoint bits, so sw(base | j << b0) = sw(base) ^ sw(j << b0)
-    unsigned o16[NV], o8[NV];
+    // disjoint bits, so sw(base | j << b0) = sw(base) ^ (XOR of sw(1 << (b0 + i)) over the
+    // set bits i of j)
+    unsigned d16[K], d8[K];
 #pragma unroll
-    for (unsigned j = 0; j < NV; ++j) {
-        o16[j] = qaoa_sw16(j << b0);
-        o8[j] = qaoa_sw8(j << b0);
+    for (unsigned i = 0; i < (unsigned)K; ++i) {
+        d16[i] = qaoa_sw16(1u << (b0 + i));
+        d8[i] = qaoa_sw8(1u << (b0 + i));
     }
+    auto off16 = [&](unsigned j) {
+        unsigned o = 0;
+#pragma unroll
+        for (unsigned i = 0; i < (unsigned)K; ++i)
+            if (j & (1u << i)) o ^= d16[i];
+        return o;
+    };
+    auto off8 = [&](unsigned j) {
+        unsigned o = 0;
+#pragma unroll
+        for (unsigned i = 0; i < (unsigned)K; ++i)
+            if (j & (1u << i)) o ^= d8[i];
+        return o;
+    };
     double acc = 0.0;
     for (unsigned r = tid; r < sets; r += nthr) {
         const unsigned base = (r & lowm) | ((r >> b0) << (b0 + K));
         const unsigned sb16 = qaoa_sw16(base), sb8 = qaoa_sw8(base);
         const idx_t xb = qaoa_index(n, P.C, P.kind, chunk, base);      // slot base | j << b0 is xb + j xs
+        // cost of element j, read from the staged words where it is used
+        auto cost_of = [&](unsigned j) -> CostT {
+            if constexpr (std::is_same<CostT, double>::value) {
+                return S.cw[sb8 ^ off8(j)];
+            } else {
+                return (CostT)((S.cw[sb8 ^ off8(j)] >> (8u * ((unsigned)(xb + j * xs) & 3u))) & 0xffu);
+            }
+        };
         double2 v[NV];
-        CostT cv[NV];
         if (sg.src == kQaoaFromSmem) {
 #pragma unroll
-            for (unsigned j = 0; j < NV; ++j) v[j] = S.vb[sb16 ^ o16[j]];
+            for (unsigned j = 0; j < NV; ++j) v[j] = S.vb[sb16 ^ off16(j)];
         } else {
 #pragma unroll
             for (unsigned j = 0; j < NV; ++j) v[j] = c2(amp0, 0.0);
-        }
-        if (need_cost) {
-            if constexpr (std::is_same<CostT, double>::value) {
-#pragma unroll
-                for (unsigned j = 0; j < NV; ++j) cv[j] = S.cw[sb8 ^ o8[j]];
-            } else {
-#pragma unroll
-                for (unsigned j = 0; j < NV; ++j)
-                    cv[j] = (CostT)((S.cw[sb8 ^ o8[j]] >> (8u * ((unsigned)(xb + j * xs) & 3u))) & 0xffu);
-            }
         }
         if (sg.pre_phase >= 0) {
             const unsigned layer = pl.layer0 + (unsigned)sg.pre_phase;
             const double gam = P.gamma[row + layer];
             const double2* tb = T.phase + (row + layer) * T.tstride;
 #pragma unroll
-            for (unsigned j = 0; j < NV; ++j) v[j] = qaoa_apply_phase(qaoa_phase<CostT>(cv[j], gam, tb), v[j]);
+            for (unsigned j = 0; j < NV; ++j) v[j] = qaoa_apply_phase(qaoa_phase<CostT>(cost_of(j), gam, tb), v[j]);
         }
         for (unsigned t = sg.t0; t <= sg.t1; ++t) {
             const unsigned layer = pl.layer0 + t;
@@ -393,7 +404,7 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
                 const double2* tb = T.phase + (row + layer + 1) * T.tstride;
 #pragma unroll
                 for (unsigned j = 0; j < NV; ++j) {
-                    const double2 ph = qaoa_phase<CostT>(cv[j], gam, tb);
+                    const double2 ph = qaoa_phase<CostT>(cost_of(j), gam, tb);
                     v[j] = qaoa_apply_phase(c2(ph.x * f, ph.y * f), v[j]);
                 }
             } else if (ends) {
@@ -404,13 +415,13 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
         }
         if (sg.dst == kQaoaToMeasure) {
 #pragma unroll
-            for (unsigned j = 0; j < NV; ++j) acc += (double)cv[j] * (v[j].x * v[j].x + v[j].y * v[j].y);
+            for (unsigned j = 0; j < NV; ++j) acc += (double)cost_of(j) * (v[j].x * v[j].x + v[j].y * v[j].y);
         } else if (sg.dst == kQaoaToGlobal) {
 #pragma unroll
             for (unsigned j = 0; j < NV; ++j) psi.st(xb + j * xs, v[j]);
         } else {
 #pragma unroll
-            for (unsigned j = 0; j < NV; ++j) S.vb[sb16 ^ o16[j]] = v[j];
+            for (unsigned j = 0; j < NV; ++j) S.vb[sb16 ^ off16(j)] = v[j];
         }
     }
     if (sg.dst == kQaoaToMeasure) S.red[tid] = acc;

@@ -147,8 +147,8 @@ def test_tune_and_cache(ork, tmp_path):
         before = bt.run(g, b)
         bt.tune(g, b, path)
         for n in ns:
-            C, t = bt.config(n)
-            assert t in (128, 256, 512) and C <= 13 and (C >= n or 2 * C >= n)
+            C, t, ring = bt.config(n)
+            assert t in (128, 256, 512) and ring in (1, 2) and C <= 13 and (C >= n or 2 * C >= n)
         after = bt.run(g, b)
         assert np.abs(after - before).max() < TOL
         lines = open(path).read().strip().splitlines()
