@@ -48,6 +48,9 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--batch-instances", type=int, default=4096, help="instances of the batched QAOA leg (0: skip)")
+    ap.add_argument("--surrogate-pairs", type=int, default=8192,
+                    help="training pairs of the surrogate leg (65536: the full configuration; 0: skip)")
     return ap.parse_args()
 
 
@@ -256,6 +259,186 @@ def run_reference(args):
     return 0
 
 
+
+# ---------------------------------------------------------------------------------------
+# batched QAOA leg: 4096 MaxCut instances of 16..24 qubits, p = 4 (include/orkan_batch.h)
+# ---------------------------------------------------------------------------------------
+def qaoa_batch_workload(count, p=4, seed=2024):
+    import numpy as np
+    from orkan_b200.batch import random_regular_graph
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(16, 25, count)
+    edges = [random_regular_graph(int(n), 3, rng) for n in ns]
+    g = rng.uniform(0, np.pi, (count, p))
+    b = rng.uniform(0, np.pi / 2, (count, p))
+    return ns, edges, g, b
+
+
+def plain_qaoa_mean(lib, n, cost, g, b):
+    """The per-call plain path (state_plus, exp_diag, rx on every qubit, mean) through a
+    library object with the reference's API: this library (GPU) or the reference (CPU)."""
+    st = lib.plus("pure", n)
+    for k in range(len(g)):
+        lib.exp_diag(st, cost, float(g[k]))
+        for q in range(n):
+            lib.gate(st, "rx", [q], 2.0 * float(b[k]))
+    m = lib.mean(st, cost)
+    lib.free(st)
+    return m
+
+
+def batched_cpu_baseline(ns, edges, g, b, budget_s):
+    """The reference library's per-call path on the host cores, timed on the smallest
+    instances of the batch; the whole batch's time is projected from the measured seconds
+    per amplitude-gate (each instance costs p (n + 1) + 2 calls over 2^n amplitudes)."""
+    import numpy as np
+    from oracle import restate as R
+    cores = host_cores()
+    lib = reference_lib(cores)
+    if lib is None:
+        return None
+    p = g.shape[1]
+    work = lambda n: (p * (n + 1) + 2) * float(2 ** n)
+    order = np.argsort(ns, kind="stable")
+    done, secs, units = 0, 0.0, 0.0
+    for i in order:
+        if secs > budget_s:
+            break
+        n = int(ns[i])
+        cost = R.maxcut_cost(n, edges[i])
+        t0 = time.perf_counter()
+        plain_qaoa_mean(lib, n, cost, g[i], b[i])
+        secs += time.perf_counter() - t0
+        units += work(n)
+        done += 1
+    total = sum(work(int(n)) for n in ns)
+    projected = secs / units * total
+    return {"value": len(ns) / projected, "unit": "evals/s", "cores": cores, "kind": "reference",
+            "sample": f"{done} instances of {int(ns[order[0]])}..{int(ns[order[done - 1]])} qubits through the "
+                      f"reference's per-call API ({secs:.1f} s), projected to the {len(ns)}-instance batch by "
+                      f"amplitude-calls, OpenMP threads = {cores}"}
+
+
+def batched_leg(args, ork, clocks_cls, local):
+    import numpy as np
+    import torch
+    from orkan_b200.batch import QaoaBatch
+    count, p = args.batch_instances, 4
+    ns, edges, g, b = qaoa_batch_workload(count, p)
+    bt = QaoaBatch(ork, ns, edges, None, p)
+    t0 = time.perf_counter()
+    bt.tune(g, b, None)
+    tune_s = time.perf_counter() - t0
+    for _ in range(max(3, args.warmup)):
+        bt.run(g, b)
+    torch.cuda.synchronize()
+    clk = clocks_cls(local)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(1, args.steps)
+    e0.record()
+    w0 = time.perf_counter()
+    for _ in range(steps):
+        means = bt.run(g, b)                # public API: host angles in, host means out
+    e1.record()
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - w0) / steps
+    ms = e0.elapsed_time(e1) / steps
+    clocks = clk.stop()
+    waves, launches = bt.stats()
+    amps = float(sum(2.0 ** int(n) for n in ns))
+    per_amp = 16 + (p - 1) * 32 + 16 + (p + 1) * 1          # state traffic of the p + 1 passes, byte costs
+    achieved = amps * per_amp / (ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    # every instance of a 64-instance sample against the per-call plain path of this library
+    rng = np.random.default_rng(5)
+    sample = rng.choice(count, 64, replace=False)
+    errs, t_plain, amps_plain = [], 0.0, 0.0
+    for i in sample:
+        cost = bt.cost_vector(int(i))
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        m = plain_qaoa_mean(ork, int(ns[i]), cost, g[i], b[i])
+        t_plain += time.perf_counter() - t1
+        amps_plain += 2.0 ** int(ns[i])
+        errs.append(abs(m - means[i]))
+    plain_evals = count / (t_plain / amps_plain * amps)
+    configs = {int(n): list(bt.config(int(n))) for n in sorted(set(int(x) for x in ns))}
+    bt.close()
+    cpu = batched_cpu_baseline(ns, edges, g, b, args.cpu_seconds) if not args.no_cpu_baseline else None
+    return {"metric": "batched evals/s", "value": count / (ms * 1e-3), "unit": "evals/s",
+            "e2e": {"value": count / wall, "unit": "evals/s", "h2d_bytes_per_step": count * p * (8 + 24),
+                    "d2h_bytes_per_step": count * 8},
+            "ms_per_batch": ms, "dtype": "f64",
+            "config": {"workload": f"{count} QAOA MaxCut instances, qubits uniform 16..24, random 3-regular graphs "
+                                   f"(one vertex of degree 2 when n is odd), p = {p}, gamma U[0, pi], beta U[0, pi/2]",
+                       "instances": count, "p": p, "waves": waves, "launches_per_run": launches,
+                       "tuned": configs, "tune_seconds": tune_s,
+                       "l2": "state vectors 1 MiB..256 MiB per instance, 62 GB per wave: larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "algorithmic_bytes_per_amplitude": per_amp},
+            "checked_vs_plain": {"instances": len(errs), "max_abs_err": max(errs), "tolerance": 1e-12},
+            "plain_per_call_gpu_evals_per_s": plain_evals,
+            "speedup_vs_plain_per_call": (count / (ms * 1e-3)) / plain_evals,
+            "cpu_baseline": cpu, "clocks": clocks}
+
+
+# ---------------------------------------------------------------------------------------
+# surrogate leg: FP32 network trained on the batched simulator's pairs, 24 qubits, p = 6
+# ---------------------------------------------------------------------------------------
+def surrogate_leg(args, ork):
+    import numpy as np
+    import torch
+    from orkan_b200.batch import erdos_renyi_graph
+    from orkan_b200.surrogate import Evaluator, Mlp, decode, encode, now, plain_sweep, surrogate_search
+    n, p, width = 24, 6, 512
+    ntrain = args.surrogate_pairs
+    rng = np.random.default_rng(77)
+    edges = erdos_renyi_graph(n, 0.3, rng)
+    w = rng.uniform(0.0, 1.0, len(edges))
+    ev = Evaluator(ork, n, edges, w, p, width)
+    t_start = now()
+    clock = lambda: now() - t_start
+    # the plain batched sweep: uniform random angles, twice the training budget
+    g, b, e, trace = plain_sweep(ev, p, 2 * ntrain, np.random.default_rng(1), width, clock)
+    t_plain_total = trace[-1][0]
+    e_plain = float(e.max())
+    target = e_plain - 1e-3
+    t_plain_hit = next(t for t, best in trace if best >= target)
+    t_data = next(t for (t, _), k in zip(trace, range(len(trace))) if (k + 1) * width >= ntrain)
+    # surrogate: the first ntrain pairs of the same sweep, then proposals until the target
+    s0 = clock()
+    best, strace, stats = surrogate_search(ork, ev, p, g[:ntrain], b[:ntrain], e[:ntrain], target, clock,
+                                           np.random.default_rng(2), epochs=60, rounds=12, proposals=1024,
+                                           ascent_steps=300)
+    s_spent = clock() - s0
+    hit = [t for t, bb in strace if bb >= target]
+    t_sur_hit = t_data + (hit[0] - s0) if hit else None
+    # surrogate error on held-out pairs (the sweep's second half), from a network trained as above
+    net = Mlp(ork, 2 * p, 256, 1024, seed=1)
+    mu, sd = float(e[:ntrain].mean()), float(e[:ntrain].std())
+    xs = torch.from_numpy(encode(g[:ntrain], b[:ntrain])).cuda()
+    ts = torch.from_numpy(((e[:ntrain] - mu) / sd).astype(np.float32)).cuda()
+    net.train(xs, ts, epochs=60, batch=1024, lr=1e-3, seed=1)
+    xh = torch.from_numpy(encode(g[ntrain:], b[ntrain:])).cuda()
+    pred = net.forward(xh).cpu().numpy().astype(np.float64) * sd + mu
+    err = pred - e[ntrain:]
+    net.close()
+    ev.close()
+    return {"metric": "surrogate vs plain time-to-|dE|<=1e-3",
+            "config": {"workload": f"{n}-qubit weighted MaxCut (Erdos-Renyi p = 0.3, {len(edges)} edges, weights "
+                                   f"U[0, 1]), p = {p} layers; FP32 MLP 12-256-256-1 GELU, Adam, batch 1024",
+                       "training_pairs": ntrain, "plain_sweep_evals": 2 * ntrain, "proposals_per_round": 1024},
+            "target": target, "plain_best": e_plain, "surrogate_best": best,
+            "plain_seconds_to_target": t_plain_hit, "plain_seconds_total": t_plain_total,
+            "surrogate_seconds_to_target": t_sur_hit,
+            "surrogate_seconds": {"data": t_data, "train": stats["train_seconds"], "search": s_spent},
+            "surrogate_rounds": stats["rounds"], "proposal_abs_err_per_round": stats["proposal_abs_err"],
+            "heldout": {"pairs": int(len(err)), "mae": float(np.mean(np.abs(err))),
+                        "rmse": float(np.sqrt(np.mean(err ** 2))),
+                        "r2": float(1.0 - np.mean(err ** 2) / np.var(e[ntrain:]))},
+            "exact_evals_per_s": len(e) / t_plain_total}
+
 # ---------------------------------------------------------------------------------------
 # this library on the GPU
 # ---------------------------------------------------------------------------------------
@@ -416,6 +599,11 @@ def run_gpu(args):
 
     for st in states.values():
         ork.free(st)
+    batched = surrogate = None
+    if rank == 0 and world == 1 and args.batch_instances > 0:
+        batched = batched_leg(args, ork, ClockSampler, local)
+    if rank == 0 and world == 1 and args.surrogate_pairs > 0:
+        surrogate = surrogate_leg(args, ork)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
@@ -429,7 +617,8 @@ def run_gpu(args):
                            "l2": "inputs larger than L2 (16 GiB and 2.15 GB states vs 126 MB L2); no flush",
                            "parallelism": f"replicas x{world}"},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-                "gpu_launches": launches, "kernel_classes": classes, "by_gate": gates}
+                "gpu_launches": launches, "kernel_classes": classes, "by_gate": gates,
+                "batched": batched, "surrogate": surrogate}
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
