@@ -51,6 +51,8 @@ def parse_args():
     ap.add_argument("--batch-instances", type=int, default=4096, help="instances of the batched QAOA leg (0: skip)")
     ap.add_argument("--surrogate-pairs", type=int, default=8192,
                     help="training pairs of the surrogate leg (65536: the full configuration; 0: skip)")
+    ap.add_argument("--noisy-pairs", type=int, default=0,
+                    help="training pairs of the noisy (density-matrix) surrogate leg (0: skip)")
     return ap.parse_args()
 
 
@@ -386,17 +388,25 @@ def batched_leg(args, ork, clocks_cls, local):
 # ---------------------------------------------------------------------------------------
 # surrogate leg: FP32 network trained on the batched simulator's pairs, 24 qubits, p = 6
 # ---------------------------------------------------------------------------------------
-def surrogate_leg(args, ork):
+def surrogate_leg(args, ork, noisy=False):
+    """Plain batched sweep vs surrogate-guided search on one cost function: the 24-qubit
+    statevector (exact evaluator: the batched simulator), or the noisy variant, a 12-qubit
+    tiled density matrix with a depolarizing channel (p = 0.01) on every qubit after each
+    mixer layer (exact evaluator: the per-call API)."""
     import numpy as np
     import torch
     from orkan_b200.batch import erdos_renyi_graph
-    from orkan_b200.surrogate import Evaluator, Mlp, decode, encode, now, plain_sweep, surrogate_search
-    n, p, width = 24, 6, 512
-    ntrain = args.surrogate_pairs
+    from orkan_b200.surrogate import (Evaluator, Mlp, NoisyEvaluator, encode, epochs_for, now, plain_sweep,
+                                      surrogate_search)
+    p = 6
+    if noisy:
+        n, width, ntrain = 12, 256, args.noisy_pairs
+    else:
+        n, width, ntrain = 24, 512, args.surrogate_pairs
     rng = np.random.default_rng(77)
     edges = erdos_renyi_graph(n, 0.3, rng)
     w = rng.uniform(0.0, 1.0, len(edges))
-    ev = Evaluator(ork, n, edges, w, p, width)
+    ev = NoisyEvaluator(ork, n, edges, w, p, 0.01) if noisy else Evaluator(ork, n, edges, w, p, width)
     t_start = now()
     clock = lambda: now() - t_start
     # the plain batched sweep: uniform random angles, twice the training budget
@@ -409,7 +419,7 @@ def surrogate_leg(args, ork):
     # surrogate: the first ntrain pairs of the same sweep, then proposals until the target
     s0 = clock()
     best, strace, stats = surrogate_search(ork, ev, p, g[:ntrain], b[:ntrain], e[:ntrain], target, clock,
-                                           np.random.default_rng(2), epochs=60, rounds=12, proposals=1024,
+                                           np.random.default_rng(2), rounds=12, proposals=min(1024, ntrain // 4),
                                            ascent_steps=300)
     s_spent = clock() - s0
     hit = [t for t, bb in strace if bb >= target]
@@ -419,21 +429,28 @@ def surrogate_leg(args, ork):
     mu, sd = float(e[:ntrain].mean()), float(e[:ntrain].std())
     xs = torch.from_numpy(encode(g[:ntrain], b[:ntrain])).cuda()
     ts = torch.from_numpy(((e[:ntrain] - mu) / sd).astype(np.float32)).cuda()
-    net.train(xs, ts, epochs=60, batch=1024, lr=1e-3, seed=1)
+    net.train(xs, ts, epochs=epochs_for(ntrain, min(1024, ntrain)), batch=min(1024, ntrain), lr=1e-3, seed=1)
     xh = torch.from_numpy(encode(g[ntrain:], b[ntrain:])).cuda()
     pred = net.forward(xh).cpu().numpy().astype(np.float64) * sd + mu
     err = pred - e[ntrain:]
     net.close()
     ev.close()
+    if noisy:
+        workload = (f"noisy variant: {n}-qubit tiled density matrix, weighted MaxCut (Erdos-Renyi p = 0.3, "
+                    f"{len(edges)} edges, weights U[0, 1]), p = {p}, depolarizing p = 0.01 on every qubit after "
+                    f"each mixer layer; FP32 MLP 12-256-256-1 GELU")
+    else:
+        workload = (f"{n}-qubit weighted MaxCut (Erdos-Renyi p = 0.3, {len(edges)} edges, weights U[0, 1]), "
+                    f"p = {p} layers; FP32 MLP 12-256-256-1 GELU, Adam, batch 1024")
     return {"metric": "surrogate vs plain time-to-|dE|<=1e-3",
-            "config": {"workload": f"{n}-qubit weighted MaxCut (Erdos-Renyi p = 0.3, {len(edges)} edges, weights "
-                                   f"U[0, 1]), p = {p} layers; FP32 MLP 12-256-256-1 GELU, Adam, batch 1024",
-                       "training_pairs": ntrain, "plain_sweep_evals": 2 * ntrain, "proposals_per_round": 1024},
+            "config": {"workload": workload, "training_pairs": ntrain, "plain_sweep_evals": 2 * ntrain,
+                       "proposals_per_round": min(1024, ntrain // 4)},
             "target": target, "plain_best": e_plain, "surrogate_best": best,
             "plain_seconds_to_target": t_plain_hit, "plain_seconds_total": t_plain_total,
             "surrogate_seconds_to_target": t_sur_hit,
             "surrogate_seconds": {"data": t_data, "train": stats["train_seconds"], "search": s_spent},
-            "surrogate_rounds": stats["rounds"], "proposal_abs_err_per_round": stats["proposal_abs_err"],
+            "surrogate_rounds": stats["rounds"], "train_loss": stats["train_loss"],
+            "proposal_abs_err_per_round": stats["proposal_abs_err"],
             "heldout": {"pairs": int(len(err)), "mae": float(np.mean(np.abs(err))),
                         "rmse": float(np.sqrt(np.mean(err ** 2))),
                         "r2": float(1.0 - np.mean(err ** 2) / np.var(e[ntrain:]))},
@@ -599,11 +616,13 @@ def run_gpu(args):
 
     for st in states.values():
         ork.free(st)
-    batched = surrogate = None
+    batched = surrogate = noisy = None
     if rank == 0 and world == 1 and args.batch_instances > 0:
         batched = batched_leg(args, ork, ClockSampler, local)
     if rank == 0 and world == 1 and args.surrogate_pairs > 0:
         surrogate = surrogate_leg(args, ork)
+    if rank == 0 and world == 1 and args.noisy_pairs > 0:
+        noisy = surrogate_leg(args, ork, noisy=True)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
@@ -618,7 +637,7 @@ def run_gpu(args):
                            "parallelism": f"replicas x{world}"},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": launches, "kernel_classes": classes, "by_gate": gates,
-                "batched": batched, "surrogate": surrogate}
+                "batched": batched, "surrogate": surrogate, "surrogate_noisy": noisy}
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

@@ -169,6 +169,56 @@ class Evaluator:
         self.batch.close()
 
 
+def depolarizing_kraus(prob):
+    """Kraus operators of the 1-qubit depolarizing channel in the p/4 form of the
+    reference's channel tests: sqrt(1 - 3p/4) I, sqrt(p/4) X, Y, Z."""
+    a, b = np.sqrt(1.0 - 3.0 * prob / 4.0), np.sqrt(prob / 4.0)
+    return [a * np.eye(2), b * np.array([[0, 1], [1, 0]]), b * np.array([[0, -1j], [1j, 0]]),
+            b * np.array([[1, 0], [0, -1]])]
+
+
+def rx_matrix(theta):
+    c, s = np.cos(theta / 2.0), np.sin(theta / 2.0)
+    return np.array([[c, -1j * s], [-1j * s, c]])
+
+
+class NoisyEvaluator:
+    """Exact FP64 <C> of the noisy circuit on a tiled density matrix through the per-call
+    API: state_plus, then per layer exp_diag(cost, gamma_k) and, on every qubit, rx(2 beta_k)
+    followed by a depolarizing channel -- applied as one channel_1q with the superoperator
+    of the Kraus set {K_i Rx} (kraus_to_superop of the library), then mean(cost)."""
+
+    def __init__(self, ork, n, edges, weights, p, prob, kind="tiled"):
+        self.ork, self.n, self.p, self.prob, self.kind = ork, n, p, prob, kind
+        x = np.arange(1 << n, dtype=np.int64)
+        cost = np.zeros(1 << n)
+        for e, (u, v) in enumerate(edges):
+            cost += (1.0 if weights is None else float(weights[e])) * (((x >> u) ^ (x >> v)) & 1)
+        self.cost = cost
+        self.kraus = depolarizing_kraus(prob)
+        self.evals = 0
+
+    def one(self, g, b):
+        ork = self.ork
+        st = ork.plus(self.kind, self.n)
+        for k in range(self.p):
+            ork.exp_diag(st, self.cost, float(g[k]))
+            rx = rx_matrix(2.0 * float(b[k]))
+            sop = ork.superop([K @ rx for K in self.kraus])
+            for q in range(self.n):
+                ork.channel_1q(st, sop, q)
+        m = ork.mean(st, self.cost)
+        ork.free(st)
+        self.evals += 1
+        return m
+
+    def __call__(self, gammas, betas):
+        return np.array([self.one(g, b) for g, b in zip(np.asarray(gammas), np.asarray(betas))])
+
+    def close(self):
+        pass
+
+
 def plain_sweep(evaluate, p, count, rng, chunk, clock):
     """The method without the network: uniformly random angles in batches; returns the
     samples, their exact values and the best-so-far trace [(seconds, best)]."""
@@ -185,7 +235,12 @@ def plain_sweep(evaluate, p, count, rng, chunk, clock):
     return np.concatenate(gs), np.concatenate(bs), np.concatenate(es), trace
 
 
-def surrogate_search(ork, evaluate, p, g, b, e, target, clock, rng, hidden=256, batch=1024, epochs=60,
+def epochs_for(count, batch=1024, steps=4000, minimum=60):
+    """Epochs giving about `steps` Adam steps (at least `minimum` epochs)."""
+    return max(minimum, int(np.ceil(steps / max(1, count // batch))))
+
+
+def surrogate_search(ork, evaluate, p, g, b, e, target, clock, rng, hidden=256, batch=1024, epochs=None,
                      rounds=8, proposals=1024, ascent_steps=300, seed=1, log=None):
     """Train the network on (angles, exact value) pairs, then repeat: propose `proposals`
     angle sets by Adam ascent on the network from the best known points and random starts,
@@ -194,6 +249,8 @@ def surrogate_search(ork, evaluate, p, g, b, e, target, clock, rng, hidden=256, 
     import torch
     dev = torch.device("cuda")
     x = encode(g, b)
+    batch = min(batch, len(e))
+    epochs = epochs_for(len(e), batch) if epochs is None else epochs
     mu, sd = float(np.mean(e)), float(np.std(e)) or 1.0
     net = Mlp(ork, n_in=2 * p, hidden=hidden, max_batch=batch, seed=seed)
     xs = torch.from_numpy(x).to(dev)

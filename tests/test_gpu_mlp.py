@@ -143,3 +143,28 @@ def test_surrogate_search_beats_plain_sweep_at_equal_exact_budget(ork):
     gg, bb = rng.uniform(0, np.pi, (1, p)), rng.uniform(0, np.pi / 2, (1, p))
     assert abs(ev(gg, bb)[0] - R.qaoa_mean(n, cost, gg[0], bb[0])) < 1e-12
     ev.close()
+
+
+def test_noisy_evaluator_matches_oracle(ork):
+    """The noisy variant's exact evaluator (tiled density matrix, rx then depolarizing on
+    every qubit per layer, fused into one superoperator per qubit) against the oracle's
+    sequential composition."""
+    from orkan_b200.batch import erdos_renyi_graph
+    from orkan_b200.surrogate import NoisyEvaluator
+    rng = np.random.default_rng(31)
+    n, p = 6, 3
+    edges = erdos_renyi_graph(n, 0.5, rng)
+    w = rng.uniform(0, 1, len(edges))
+    ev = NoisyEvaluator(ork, n, edges, w, p, 0.01)
+    g, b = rng.uniform(0, np.pi, (2, p)), rng.uniform(0, np.pi / 2, (2, p))
+    got = ev(g, b)
+    cost = R.maxcut_cost(n, edges, w)
+    sop = R.kraus_to_superop(R.depolarizing_kraus(0.01))
+    for i in range(2):
+        rho = R.plus_state("tiled", n)
+        for k in range(p):
+            rho = R.exp_diag("tiled", rho, cost, g[i, k])
+            for q in range(n):
+                rho = R.apply_gate("tiled", rho, "rx", [q], 2 * b[i, k])
+                rho = R.apply_superop1(rho, sop, q)
+        assert abs(got[i] - R.mean("tiled", rho, cost)) < 1e-12
