@@ -396,7 +396,7 @@ def surrogate_leg(args, ork, noisy=False):
     import numpy as np
     import torch
     from orkan_b200.batch import erdos_renyi_graph
-    from orkan_b200.surrogate import (Evaluator, Mlp, NoisyEvaluator, encode, epochs_for, now, plain_sweep,
+    from orkan_b200.surrogate import (Evaluator, Mlp, NoisyEvaluator, encode, fit, now, plain_sweep,
                                       surrogate_search)
     p = 6
     if noisy:
@@ -407,29 +407,38 @@ def surrogate_leg(args, ork, noisy=False):
     edges = erdos_renyi_graph(n, 0.3, rng)
     w = rng.uniform(0.0, 1.0, len(edges))
     ev = NoisyEvaluator(ork, n, edges, w, p, 0.01) if noisy else Evaluator(ork, n, edges, w, p, width)
+    rounds, proposals = 8, min(1024, ntrain // 8)
     t_start = now()
     clock = lambda: now() - t_start
     # the plain batched sweep: uniform random angles, twice the training budget
     g, b, e, trace = plain_sweep(ev, p, 2 * ntrain, np.random.default_rng(1), width, clock)
     t_plain_total = trace[-1][0]
     e_plain = float(e.max())
-    target = e_plain - 1e-3
-    t_plain_hit = next(t for t, best in trace if best >= target)
-    t_data = next(t for (t, _), k in zip(trace, range(len(trace))) if (k + 1) * width >= ntrain)
-    # surrogate: the first ntrain pairs of the same sweep, then proposals until the target
-    s0 = clock()
-    best, strace, stats = surrogate_search(ork, ev, p, g[:ntrain], b[:ntrain], e[:ntrain], target, clock,
-                                           np.random.default_rng(2), rounds=12, proposals=min(1024, ntrain // 4),
-                                           ascent_steps=300)
-    s_spent = clock() - s0
-    hit = [t for t, bb in strace if bb >= target]
-    t_sur_hit = t_data + (hit[0] - s0) if hit else None
-    # surrogate error on held-out pairs (the sweep's second half), from a network trained as above
+    k_data = next(k for k in range(len(trace)) if (k + 1) * width >= ntrain)
+    t_data = trace[k_data][0]
+    # surrogate-guided search: the same sweep's first ntrain pairs, then proposal rounds
+    # (its best-so-far trace is the sweep's up to t_data, then its own rounds); the same
+    # rounds without the network are the ablation
+    def search(use_network):
+        s0 = clock()
+        best, strace, stats = surrogate_search(ork, ev, p, g[:ntrain], b[:ntrain], e[:ntrain], np.inf, clock,
+                                               np.random.default_rng(2), rounds=rounds, proposals=proposals,
+                                               use_network=use_network)
+        return best, trace[:k_data + 1] + [(t_data + (t - s0), bb) for t, bb in strace], stats, clock() - s0
+
+    best, sur_trace, stats, s_spent = search(True)
+    best_abl, abl_trace, _, _ = search(False)
+
+    def time_to(tr, level):
+        hit = [t for t, bb in tr if bb >= level]
+        return hit[0] if hit else None
+
+    target_plain = e_plain - 1e-3
+    target_best = max(e_plain, best) - 1e-3
+    # surrogate error on held-out pairs (the sweep's second half), network trained as above
     net = Mlp(ork, 2 * p, 256, 1024, seed=1)
     mu, sd = float(e[:ntrain].mean()), float(e[:ntrain].std())
-    xs = torch.from_numpy(encode(g[:ntrain], b[:ntrain])).cuda()
-    ts = torch.from_numpy(((e[:ntrain] - mu) / sd).astype(np.float32)).cuda()
-    net.train(xs, ts, epochs=epochs_for(ntrain, min(1024, ntrain)), batch=min(1024, ntrain), lr=1e-3, seed=1)
+    fit(net, encode(g[:ntrain], b[:ntrain]), (e[:ntrain] - mu) / sd, seed=1)
     xh = torch.from_numpy(encode(g[ntrain:], b[ntrain:])).cuda()
     pred = net.forward(xh).cpu().numpy().astype(np.float64) * sd + mu
     err = pred - e[ntrain:]
@@ -444,12 +453,18 @@ def surrogate_leg(args, ork, noisy=False):
                     f"p = {p} layers; FP32 MLP 12-256-256-1 GELU, Adam, batch 1024")
     return {"metric": "surrogate vs plain time-to-|dE|<=1e-3",
             "config": {"workload": workload, "training_pairs": ntrain, "plain_sweep_evals": 2 * ntrain,
-                       "proposals_per_round": min(1024, ntrain // 4)},
-            "target": target, "plain_best": e_plain, "surrogate_best": best,
-            "plain_seconds_to_target": t_plain_hit, "plain_seconds_total": t_plain_total,
-            "surrogate_seconds_to_target": t_sur_hit,
+                       "proposals_per_round": proposals, "rounds": stats["rounds"]},
+            "plain_best": e_plain, "surrogate_best": best, "no_network_best": best_abl,
+            "target_plain_best": {"level": target_plain, "plain_seconds": time_to(trace, target_plain),
+                                  "surrogate_seconds": time_to(sur_trace, target_plain),
+                                  "no_network_seconds": time_to(abl_trace, target_plain)},
+            "target_overall_best": {"level": target_best, "plain_seconds": time_to(trace, target_best),
+                                    "surrogate_seconds": time_to(sur_trace, target_best),
+                                    "no_network_seconds": time_to(abl_trace, target_best),
+                                    "plain_budget_seconds": t_plain_total},
             "surrogate_seconds": {"data": t_data, "train": stats["train_seconds"], "search": s_spent},
-            "surrogate_rounds": stats["rounds"], "train_loss": stats["train_loss"],
+            "exact_evals": {"plain": int(len(e)), "surrogate": int(ntrain + proposals * stats["rounds"])},
+            "local_validation_r2_per_round": stats["validation_r2"], "radius_per_round": stats["radius"],
             "proposal_abs_err_per_round": stats["proposal_abs_err"],
             "heldout": {"pairs": int(len(err)), "mae": float(np.mean(np.abs(err))),
                         "rmse": float(np.sqrt(np.mean(err ** 2))),

@@ -240,58 +240,99 @@ def epochs_for(count, batch=1024, steps=4000, minimum=60):
     return max(minimum, int(np.ceil(steps / max(1, count // batch))))
 
 
-def surrogate_search(ork, evaluate, p, g, b, e, target, clock, rng, hidden=256, batch=1024, epochs=None,
-                     rounds=8, proposals=1024, ascent_steps=300, seed=1, log=None):
-    """Train the network on (angles, exact value) pairs, then repeat: propose `proposals`
-    angle sets by Adam ascent on the network from the best known points and random starts,
-    re-score them exactly, add them to the training set and fine-tune; stop once an exactly
-    scored proposal reaches `target`.  Returns (best exact value, seconds, trace, stats)."""
+def fit(net, x, t, batch=1024, lr=1e-3, seed=0, chunk_epochs=5, patience=4, max_epochs=None, val_frac=0.1):
+    """Train with early stopping: a fixed 10 % of the pairs is held out, the network trains
+    in chunks of `chunk_epochs` epochs on the rest, and the parameters with the lowest
+    held-out error are kept.  x, t: numpy arrays (t already normalised).  Returns
+    (held-out MSE, epochs trained)."""
     import torch
     dev = torch.device("cuda")
-    x = encode(g, b)
-    batch = min(batch, len(e))
-    epochs = epochs_for(len(e), batch) if epochs is None else epochs
-    mu, sd = float(np.mean(e)), float(np.std(e)) or 1.0
-    net = Mlp(ork, n_in=2 * p, hidden=hidden, max_batch=batch, seed=seed)
-    xs = torch.from_numpy(x).to(dev)
-    ts = torch.from_numpy(((e - mu) / sd).astype(np.float32)).to(dev)
-    stats = {"train_samples": len(e), "epochs": epochs}
-    t0 = clock()
-    loss = net.train(xs, ts, epochs=epochs, batch=batch, lr=1e-3, seed=seed)
-    stats["train_seconds"] = clock() - t0
-    stats["train_loss"] = loss
-    # surrogate error on held-out exact points (fresh uniform samples are not needed: the
-    # proposals below are exactly scored, and their prediction error is recorded per round)
-    best = float(np.max(e))
+    n = len(t)
+    idx = np.random.default_rng(seed).permutation(n)
+    nv = max(1, int(n * val_frac))
+    tr, va = idx[nv:], idx[:nv]
+    batch = min(batch, len(tr))
+    xs = torch.from_numpy(np.ascontiguousarray(x[tr])).to(dev)
+    ts = torch.from_numpy(np.ascontiguousarray(t[tr]).astype(np.float32)).to(dev)
+    xv = torch.from_numpy(np.ascontiguousarray(x[va])).to(dev)
+    tv = t[va].astype(np.float64)
+    max_epochs = max_epochs or epochs_for(len(tr), batch)
+    best, best_p, bad, done = np.inf, net.get_params(), 0, 0
+    while done < max_epochs and bad < patience:
+        net.train(xs, ts, epochs=chunk_epochs, batch=batch, lr=lr, seed=seed + done)
+        done += chunk_epochs
+        mse = float(np.mean((net.forward(xv).cpu().numpy().astype(np.float64) - tv) ** 2))
+        if mse < best:
+            best, best_p, bad = mse, net.get_params(), 0
+        else:
+            bad += 1
+    net.set_params(best_p)
+    return best, done
+
+
+def surrogate_search(ork, evaluate, p, g, b, e, target, clock, rng, hidden=256, batch=1024, rounds=8,
+                     proposals=1024, local=4096, radius=0.25, screen=32, seed=1, use_network=True, log=None):
+    """Surrogate-guided trust-region search from exactly scored pairs (angles g, b -> e).
+
+    Every round fits the network (early stopping on a held-out 10 %) to the `local` pairs
+    nearest to the best point so far -- the landscape is smooth at that scale even where it
+    is not over the whole angle box -- draws `screen` x `proposals` candidates uniformly in
+    the box of half width `radius` (input units) around that point, keeps the `proposals`
+    the network ranks highest, and re-scores them exactly in FP64.  The radius grows after
+    a round that improved the best value and shrinks after one that did not.  With
+    use_network=False the first `proposals` candidates are scored as drawn (the same search
+    without the network).  Stops when the best exact value reaches `target`.
+    Returns (best exact value, trace [(seconds, best)], stats)."""
+    import torch
+    dev = torch.device("cuda")
+    all_x = encode(g, b)
+    all_e = np.asarray(e, dtype=np.float64)
+    net = Mlp(ork, n_in=2 * p, hidden=hidden, max_batch=batch, seed=seed) if use_network else None
+    stats = {"train_samples": len(all_e), "train_seconds": 0.0, "validation_r2": [], "epochs": [],
+             "radius": [], "proposal_abs_err": []}
+    best_i = int(np.argmax(all_e))
+    best = float(all_e[best_i])
     trace = [(clock(), best)]
-    all_x, all_e = x, e
-    errs = []
+    rad = radius
     for r in range(rounds):
-        order = np.argsort(-all_e)
-        n_top = proposals // 2
-        starts = all_x[order[:n_top]] + rng.normal(0, 0.05, (n_top, 2 * p)).astype(np.float32)
-        starts = np.concatenate([starts, rng.uniform(-1, 1, (proposals - n_top, 2 * p)).astype(np.float32)])
-        xp = torch.from_numpy(np.clip(starts, -1, 1).astype(np.float32)).to(dev)
-        pred = net.ascend(xp, steps=ascent_steps, lr=0.02)
-        xq = xp.cpu().numpy()
+        center = all_x[best_i]
+        d = np.max(np.abs(all_x - center), axis=1)
+        near = np.argsort(d)[:local]
+        lo, hi = np.maximum(center - rad, -1.0), np.minimum(center + rad, 1.0)
+        cand = rng.uniform(lo, hi, (screen * proposals, 2 * p)).astype(np.float32)
+        stats["radius"].append(rad)
+        if net is not None:
+            t0 = clock()
+            ee = all_e[near]
+            mu, sd = float(ee.mean()), float(ee.std()) or 1.0
+            val_mse, ep = fit(net, all_x[near], (ee - mu) / sd, batch=min(batch, len(near)), seed=seed + r)
+            stats["train_seconds"] += clock() - t0
+            stats["validation_r2"].append(1.0 - val_mse)
+            stats["epochs"].append(ep)
+            y = net.forward(torch.from_numpy(cand).to(dev)).cpu().numpy().astype(np.float64)
+            top = np.argsort(-y)[:proposals]
+            xq, pred = cand[top], y[top] * sd + mu
+        else:
+            xq, pred = cand[:proposals], None
         gq, bq = decode(xq, p)
         eq = evaluate(gq, bq)
-        pq = pred.cpu().numpy().astype(np.float64) * sd + mu
-        errs.append(float(np.mean(np.abs(pq - eq))))
-        best = max(best, float(eq.max()))
-        trace.append((clock(), best))
-        if log:
-            log(f"round {r}: best exact {best:.6f}, proposals max {eq.max():.6f}, |pred - exact| mean {errs[-1]:.4f}")
+        if pred is not None:
+            stats["proposal_abs_err"].append(float(np.mean(np.abs(pred - eq))))
+        improved = float(eq.max()) > best
         all_x = np.concatenate([all_x, xq])
         all_e = np.concatenate([all_e, eq])
+        if improved:
+            best_i = int(np.argmax(all_e))
+            best = float(all_e[best_i])
+        rad = min(1.0, rad * 1.5) if improved else max(0.02, rad * 0.5)
+        trace.append((clock(), best))
+        if log:
+            log(f"round {r}: best exact {best:.6f}, radius {rad:.3f}")
         if best >= target:
             break
-        xs = torch.from_numpy(all_x).to(dev)
-        ts = torch.from_numpy(((all_e - mu) / sd).astype(np.float32)).to(dev)
-        net.train(xs, ts, epochs=max(2, epochs // 6), batch=batch, lr=3e-4, seed=seed + r + 1)
-    stats["proposal_abs_err"] = errs
-    stats["rounds"] = len(errs)
-    net.close()
+    stats["rounds"] = len(trace) - 1
+    if net is not None:
+        net.close()
     return best, trace, stats
 
 

@@ -117,10 +117,11 @@ def test_ascent_increases_the_prediction(ork, torch):
     net.close()
 
 
-def test_surrogate_search_beats_plain_sweep_at_equal_exact_budget(ork):
-    """The network's gain over the method without it: with the same number of exact
-    evaluations, the surrogate-guided search (half the budget as training data from the
-    sweep, half as re-scored proposals) finds a higher exact <C> than the plain sweep."""
+def test_surrogate_search_beats_plain_sweep_and_its_ablation(ork):
+    """The network's gain: with the same exact-evaluation budget (half of it the sweep's
+    first pairs, the rest re-scored proposals), the surrogate-guided search finds a higher
+    exact <C> than the plain sweep, and than the same trust-region rounds without the
+    network (starts scored as drawn)."""
     from orkan_b200.batch import erdos_renyi_graph
     from orkan_b200.surrogate import Evaluator, now, plain_sweep, surrogate_search
     rng = np.random.default_rng(21)
@@ -132,12 +133,13 @@ def test_surrogate_search_beats_plain_sweep_at_equal_exact_budget(ork):
     g, b, e, _ = plain_sweep(ev, p, budget, np.random.default_rng(1), 1024, now)
     plain_best = float(e.max())
     half = budget // 2
-    best, trace, stats = surrogate_search(ork, ev, p, g[:half], b[:half], e[:half], target=np.inf, clock=now,
-                                          rng=np.random.default_rng(2), epochs=60, rounds=4, proposals=1024,
-                                          ascent_steps=200)
-    used = half + 1024 * stats["rounds"]
-    assert used <= budget
+    kw = dict(target=np.inf, clock=now, rounds=8, proposals=512)
+    best, _, stats = surrogate_search(ork, ev, p, g[:half], b[:half], e[:half], rng=np.random.default_rng(2), **kw)
+    best_abl, _, _ = surrogate_search(ork, ev, p, g[:half], b[:half], e[:half], rng=np.random.default_rng(2),
+                                      use_network=False, **kw)
+    assert half + 512 * stats["rounds"] <= budget
     assert best > plain_best + 1e-3, (best, plain_best)
+    assert best > best_abl, (best, best_abl)
     # the proposals' exact values are the FP64 simulator's: spot-check one against the oracle
     cost = R.maxcut_cost(n, edges, w)
     gg, bb = rng.uniform(0, np.pi, (1, p)), rng.uniform(0, np.pi / 2, (1, p))
