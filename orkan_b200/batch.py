@@ -137,3 +137,54 @@ def random_regular_graph(n: int, d: int, rng) -> list[tuple[int, int]]:
 
 def erdos_renyi_graph(n: int, prob: float, rng) -> list[tuple[int, int]]:
     return [(u, v) for u in range(n) for v in range(u + 1, n) if rng.random() < prob]
+
+
+def _main(argv=None):
+    """Run one batch of 3-regular MaxCut instances: python -m orkan_b200.batch --count 64
+    --qubits 20 [--p 4 --chunk 12 --threads 256 --ring 1 --runs 2].  With --chunk the
+    launch configuration of that qubit count is set through a tuner cache file instead of
+    tuning.  Prints the configuration, the first mean and the time per run."""
+    import argparse
+    import json
+    import os
+    import tempfile
+    import time
+
+    import orkan_b200
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--count", type=int, default=64)
+    ap.add_argument("--qubits", type=int, default=20)
+    ap.add_argument("--p", type=int, default=4)
+    ap.add_argument("--chunk", type=int, default=0)
+    ap.add_argument("--threads", type=int, default=256)
+    ap.add_argument("--ring", type=int, default=1)
+    ap.add_argument("--runs", type=int, default=2)
+    ap.add_argument("--f64", action="store_true")
+    a = ap.parse_args(argv)
+    ork = orkan_b200.load(5)
+    rng = np.random.default_rng(5)
+    edges = [random_regular_graph(a.qubits, 3, rng) for _ in range(a.count)]
+    g = rng.uniform(0, np.pi, (a.count, a.p))
+    b = rng.uniform(0, np.pi / 2, (a.count, a.p))
+    bt = QaoaBatch(ork, [a.qubits] * a.count, edges, None, a.p, f64_costs=a.f64)
+    if a.chunk:
+        import torch
+        key = f"{torch.cuda.get_device_name()}|n{a.qubits}|p{a.p}|{'f64' if a.f64 else 'u8'}"
+        fd, path = tempfile.mkstemp(suffix=".json")
+        with os.fdopen(fd, "w") as f:
+            f.write(json.dumps({key: {"C": a.chunk, "threads": a.threads, "ring": a.ring}}) + "\n")
+        bt.tune(g, b, path)
+        os.unlink(path)
+    means = bt.run(g, b)
+    t0 = time.perf_counter()
+    for _ in range(a.runs):
+        means = bt.run(g, b)
+    dt = (time.perf_counter() - t0) / max(1, a.runs)
+    print(json.dumps({"config": bt.config(a.qubits), "stats": bt.stats(), "mean0": float(means[0]),
+                      "ms_per_run": dt * 1e3}))
+    bt.close()
+
+
+if __name__ == "__main__":
+    _main()

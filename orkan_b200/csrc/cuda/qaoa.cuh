@@ -16,15 +16,16 @@
 // (x = row * 2^C + col), so the qubits it mixes are local in both.  Instances with n <= C
 // run the whole circuit in one pass ("full") and never touch a state vector in memory.
 //
-// Inside a work item the mixer runs in register stages of up to kQaoaGroup qubits (every
-// thread holds 2^k amplitudes that differ only in the group's bits and applies the group's
-// butterflies in registers); between stages the chunk sits in shared memory.  Rx on
-// different qubits commute, so the order of the groups is free: the first stage of a pass
-// loads its amplitudes straight from device memory and the last one stores them (or
-// measures), both with a group whose bits exclude the low slot bits, so that consecutive
-// lanes touch consecutive amplitudes; and segment t + 1 starts with the group segment t
-// ended with, so that stage applies segment t's butterflies, the phase between the
-// segments and segment t + 1's butterflies without going back to shared memory.
+// Inside a work item the chunk is copied into shared memory asynchronously, and the mixer
+// runs in register stages of up to kQaoaGroup qubits (every thread holds 2^k amplitudes that
+// differ only in the group's bits and applies the group's butterflies in registers); the
+// slots of a high chunk are numbered rows first, so every group starts at slot bit 0, 4, 8
+// or 12.  Rx on different qubits commute, so the order of the groups is free: the last
+// stage of a pass stores from registers (or measures) with the group of the highest bits,
+// so that consecutive lanes touch consecutive amplitudes of a low chunk; and segment t + 1
+// starts with the group segment t ended with, so that stage applies segment t's butterflies,
+// the phase between the segments and segment t + 1's butterflies without going back to
+// shared memory.
 //
 // Arithmetic (checked against the per-call path at 1e-12): the rx pair update
 // (a, b) -> (c a - i s b, c b - i s a) with c = cos(beta), s = sin(beta) (rx(2 beta) of
@@ -103,23 +104,26 @@ ORKAN_HD unsigned qaoa_lc(unsigned n, unsigned C, unsigned kind) { return kind =
 // log2 of the number of columns a high chunk spans
 ORKAN_HD unsigned qaoa_logw(unsigned n, unsigned C) { return 2 * C - n; }
 
-// Global amplitude index of slot s of chunk c.
+// Global amplitude index of slot s of chunk c.  Low chunk: x = c 2^C + s.  High chunk
+// (rows-first): s = row + col 2^R with R = n - C row bits, x = row 2^C + c W + col.
 ORKAN_HD idx_t qaoa_index(unsigned n, unsigned C, unsigned kind, idx_t c, unsigned s) {
     if (kind == kQaoaFull) return s;
     if (kind == kQaoaLow) return (c << C) + s;
-    const unsigned lw = qaoa_logw(n, C);
-    const unsigned row = s >> lw, col = s & ((1u << lw) - 1);
+    const unsigned R = n - C, lw = qaoa_logw(n, C);
+    const unsigned row = s & ((1u << R) - 1), col = s >> R;
     return ((idx_t)row << C) + (c << lw) + col;
 }
 
-// Index distance of slot bit b (a mixer qubit's bit: a row bit in high passes).
+// Index distance of slot bit b of a mixed qubit (a row bit in high passes).
 ORKAN_HD idx_t qaoa_stride(unsigned n, unsigned C, unsigned kind, unsigned b) {
-    return kind == kQaoaHigh ? idx_t(1) << (b - qaoa_logw(n, C) + C) : idx_t(1) << b;
+    (void)n;
+    return kind == kQaoaHigh ? idx_t(1) << (b + C) : idx_t(1) << b;
 }
 
 // Slot bit of qubit q.
 ORKAN_HD unsigned qaoa_bit(unsigned n, unsigned C, unsigned kind, unsigned q) {
-    return kind == kQaoaHigh ? q - C + qaoa_logw(n, C) : q;
+    (void)n;
+    return kind == kQaoaHigh ? q - C : q;
 }
 
 // Work item w -> position in the pass's instance list (binary search over item0).
@@ -133,10 +137,13 @@ ORKAN_HD unsigned qaoa_find(const QaoaInst* inst, unsigned ninst, idx_t w) {
     return lo;
 }
 
-// Shared-memory slot permutations that keep the register stages free of bank conflicts
-// for every group position (16-byte amplitudes; 8-byte and 4-byte cost words).
-ORKAN_HD unsigned qaoa_sw16(unsigned s) { return s ^ ((s >> 4) & 7u); }
-ORKAN_HD unsigned qaoa_sw8(unsigned s) { return s ^ ((s >> 4) & 15u); }
+// Shared-memory position of slot s: one padding slot after every 16.  With the mixed qubits
+// in groups of 4 slot bits starting at bit 0, 4, 8 or 12, the slots of a register set are
+// then equally spaced (base + j 2^b0 sits at pad(base) + j (2^b0 + 2^(b0-4)), or + j for
+// b0 = 0), and the lanes of a warp, which differ in the lowest non-group bits, fall in
+// distinct banks for every group position and element size.
+ORKAN_HD unsigned qaoa_pad(unsigned s) { return s + (s >> 4); }
+ORKAN_HD unsigned qaoa_padded(unsigned C) { return (1u << C) + (1u << C) / 16; }
 
 // What one pass does.
 struct QaoaPlan {
@@ -255,7 +262,7 @@ struct QaoaSmem {
 
 template <class CostT>
 ORKAN_HD size_t qaoa_buffer_bytes(unsigned C) {
-    return (size_t(16) + sizeof(typename QaoaCostWord<CostT>::type)) * (size_t(1) << C);
+    return (size_t(16) + sizeof(typename QaoaCostWord<CostT>::type)) * qaoa_padded(C);
 }
 template <class CostT>
 ORKAN_HD size_t qaoa_smem_bytes(unsigned C, unsigned nthr, unsigned ring) {
@@ -266,21 +273,10 @@ ORKAN_HD QaoaSmem<CostT> qaoa_smem_at(unsigned char* base, unsigned C, unsigned 
     QaoaSmem<CostT> S;
     unsigned char* b = base + qaoa_buffer_bytes<CostT>(C) * slot;
     S.vb = reinterpret_cast<double2*>(b);
-    S.cw = reinterpret_cast<typename QaoaCostWord<CostT>::type*>(b + size_t(16) * (size_t(1) << C));
+    S.cw = reinterpret_cast<typename QaoaCostWord<CostT>::type*>(b + size_t(16) * qaoa_padded(C));
     S.red = reinterpret_cast<double*>(base + qaoa_buffer_bytes<CostT>(C) * ring);
     (void)nthr;
     return S;
-}
-
-// Cost of slot s (global index x) from its staged word.
-template <class CostT>
-ORKAN_HD CostT qaoa_cost_at(const QaoaSmem<CostT>& S, unsigned s, idx_t x) {
-    if constexpr (std::is_same<CostT, double>::value) {
-        (void)x;
-        return S.cw[qaoa_sw8(s)];
-    } else {
-        return (CostT)((S.cw[qaoa_sw8(s)] >> (8u * ((unsigned)x & 3u))) & 0xffu);
-    }
 }
 
 // Fill of one work item's buffer: asynchronous copies of its amplitudes (unless the pass
@@ -293,8 +289,8 @@ ORKAN_HD void qaoa_fill(const QaoaPass& P, const QaoaInst& I, const QaoaPlan& pl
     const unsigned cnt = 1u << qaoa_lc(I.n, P.C, P.kind);
     for (unsigned s = tid; s < cnt; s += nthr) {
         const idx_t x = qaoa_index(I.n, P.C, P.kind, chunk, s);
-        if (!pl.init) psi.cp16(S.vb + qaoa_sw16(s), x);
-        cost.cpw(S.cw + qaoa_sw8(s), x);
+        if (!pl.init) psi.cp16(S.vb + qaoa_pad(s), x);
+        cost.cpw(S.cw + qaoa_pad(s), x);
     }
 }
 
@@ -304,59 +300,37 @@ ORKAN_HD double qaoa_powu(double x, unsigned e) {
     return r;
 }
 
-// Register stage of a group of K slot bits starting at b0.
-template <int K, class CostT, class Mem>
+// Register stage of a group of K slot bits starting at B0 (0, 4, 8 or 12).
+template <int K, int B0, class CostT, class Mem>
 ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst& I, const QaoaPlan& pl,
                          const QaoaStage& sg, const Mem& psi, idx_t chunk, const QaoaSmem<CostT>& S, unsigned lc,
-                         unsigned b0, unsigned tid, unsigned nthr) {
+                         unsigned tid, unsigned nthr) {
     constexpr unsigned NV = 1u << K;
+    constexpr unsigned D = B0 == 0 ? 1u : (1u << B0) + (1u << (B0 - 4));   // padded distance of element j
+    constexpr unsigned LOWM = (1u << B0) - 1;
     const unsigned n = I.n;
     const unsigned sets = 1u << (lc - K);
-    const unsigned lowm = (1u << b0) - 1;
-    const idx_t xs = qaoa_stride(n, P.C, P.kind, b0);
+    const idx_t xs = qaoa_stride(n, P.C, P.kind, B0);
     const unsigned nq = pl.q1 - pl.q0;
     const idx_t row = (idx_t)I.pos * P.p;
     const double amp0 = 1.0 / sqrt((double)(idx_t(1) << n));
-    // shared-memory slot of element j: the swizzles are XOR-linear and base, j << b0 have
-    // disjoint bits, so sw(base | j << b0) = sw(base) ^ (XOR of sw(1 << (b0 + i)) over the
-    // set bits i of j)
-    unsigned d16[K], d8[K];
-#pragma unroll
-    for (unsigned i = 0; i < (unsigned)K; ++i) {
-        d16[i] = qaoa_sw16(1u << (b0 + i));
-        d8[i] = qaoa_sw8(1u << (b0 + i));
-    }
-    auto off16 = [&](unsigned j) {
-        unsigned o = 0;
-#pragma unroll
-        for (unsigned i = 0; i < (unsigned)K; ++i)
-            if (j & (1u << i)) o ^= d16[i];
-        return o;
-    };
-    auto off8 = [&](unsigned j) {
-        unsigned o = 0;
-#pragma unroll
-        for (unsigned i = 0; i < (unsigned)K; ++i)
-            if (j & (1u << i)) o ^= d8[i];
-        return o;
-    };
     double acc = 0.0;
     for (unsigned r = tid; r < sets; r += nthr) {
-        const unsigned base = (r & lowm) | ((r >> b0) << (b0 + K));
-        const unsigned sb16 = qaoa_sw16(base), sb8 = qaoa_sw8(base);
-        const idx_t xb = qaoa_index(n, P.C, P.kind, chunk, base);      // slot base | j << b0 is xb + j xs
+        const unsigned base = (r & LOWM) | ((r >> B0) << (B0 + K));
+        const unsigned p0 = qaoa_pad(base);
+        const idx_t xb = qaoa_index(n, P.C, P.kind, chunk, base);      // slot base | j << B0 is xb + j xs
         // cost of element j, read from the staged words where it is used
         auto cost_of = [&](unsigned j) -> CostT {
             if constexpr (std::is_same<CostT, double>::value) {
-                return S.cw[sb8 ^ off8(j)];
+                return S.cw[p0 + j * D];
             } else {
-                return (CostT)((S.cw[sb8 ^ off8(j)] >> (8u * ((unsigned)(xb + j * xs) & 3u))) & 0xffu);
+                return (CostT)((S.cw[p0 + j * D] >> (8u * ((unsigned)(xb + j * xs) & 3u))) & 0xffu);
             }
         };
         double2 v[NV];
         if (sg.src == kQaoaFromSmem) {
 #pragma unroll
-            for (unsigned j = 0; j < NV; ++j) v[j] = S.vb[sb16 ^ off16(j)];
+            for (unsigned j = 0; j < NV; ++j) v[j] = S.vb[p0 + j * D];
         } else {
 #pragma unroll
             for (unsigned j = 0; j < NV; ++j) v[j] = c2(amp0, 0.0);
@@ -421,7 +395,7 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
             for (unsigned j = 0; j < NV; ++j) psi.st(xb + j * xs, v[j]);
         } else {
 #pragma unroll
-            for (unsigned j = 0; j < NV; ++j) S.vb[sb16 ^ off16(j)] = v[j];
+            for (unsigned j = 0; j < NV; ++j) S.vb[p0 + j * D] = v[j];
         }
     }
     if (sg.dst == kQaoaToMeasure) S.red[tid] = acc;
@@ -440,13 +414,17 @@ ORKAN_HD void qaoa_stage(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
         const unsigned nq = pl.q1 - pl.q0;
         const unsigned off = sg.g * kQaoaGroup;
         const unsigned k = (nq - off) < kQaoaGroup ? nq - off : kQaoaGroup;
-        const unsigned b0 = qaoa_bit(n, P.C, kind, pl.q0 + off);
-        switch (k) {
-            case 1: qaoa_group<1, CostT>(P, T, I, pl, sg, psi, chunk, S, lc, b0, tid, nthr); break;
-            case 2: qaoa_group<2, CostT>(P, T, I, pl, sg, psi, chunk, S, lc, b0, tid, nthr); break;
-            case 3: qaoa_group<3, CostT>(P, T, I, pl, sg, psi, chunk, S, lc, b0, tid, nthr); break;
-            default: qaoa_group<4, CostT>(P, T, I, pl, sg, psi, chunk, S, lc, b0, tid, nthr); break;
+        const unsigned b0 = qaoa_bit(n, P.C, kind, pl.q0 + off);     // 0, 4, 8 or 12
+#define ORKAN_QAOA_GROUP(KK, BB) \
+    case (KK) * 16 + (BB): qaoa_group<KK, BB, CostT>(P, T, I, pl, sg, psi, chunk, S, lc, tid, nthr); break;
+        switch (k * 16 + b0) {
+            ORKAN_QAOA_GROUP(1, 0) ORKAN_QAOA_GROUP(2, 0) ORKAN_QAOA_GROUP(3, 0) ORKAN_QAOA_GROUP(4, 0)
+            ORKAN_QAOA_GROUP(1, 4) ORKAN_QAOA_GROUP(2, 4) ORKAN_QAOA_GROUP(3, 4) ORKAN_QAOA_GROUP(4, 4)
+            ORKAN_QAOA_GROUP(1, 8) ORKAN_QAOA_GROUP(2, 8) ORKAN_QAOA_GROUP(3, 8) ORKAN_QAOA_GROUP(4, 8)
+            ORKAN_QAOA_GROUP(1, 12) ORKAN_QAOA_GROUP(2, 12) ORKAN_QAOA_GROUP(3, 12) ORKAN_QAOA_GROUP(4, 12)
+            default: break;
         }
+#undef ORKAN_QAOA_GROUP
         return;
     }
     // fold of the per-thread sums in a fixed order: 32 strided partial sums, then one

@@ -64,6 +64,20 @@ def test_passes_match_oracle_prefixes(n, C, p):
             assert abs(m - R.qaoa_mean(n, cost, g, b)) < 1e-12
 
 
+@pytest.mark.parametrize("n,C,nthr", [(14, 13, 512), (13, 13, 512), (20, 12, 256), (17, 11, 128)])
+def test_bench_chunk_shapes(n, C, nthr):
+    """Chunk shapes of the GPU configurations: 2^13 chunks (a one-qubit group at slot bit
+    12), 2^12 and 2^11 chunks with high passes of 8 and 6 row bits."""
+    edges, _ = graph(n, 5)
+    cost = R.maxcut_cost(n, edges)
+    g, b = angles(2, 11)
+    res, m = kemu.qaoa(n, cost, 2, g, b, log_chunk=C, nthr=nthr, byte_cost=True)
+    assert res.oob == 0
+    if n > C:
+        assert np.all(res.writes == 2) and np.all(res.reads == 2)
+    assert abs(m - R.qaoa_mean(n, cost, g, b)) < 1e-12
+
+
 @pytest.mark.parametrize("nthr", [32, 96, 256])
 def test_thread_counts(nthr):
     n, C, p = 10, 6, 3
