@@ -260,9 +260,25 @@ struct QaoaSmem {
     double* red;
 };
 
+// Bytes of one buffer, rounded up to 128 so that every buffer, its cost words and the
+// reduction array after the last buffer keep the alignment of the shared-memory base.
 template <class CostT>
 ORKAN_HD size_t qaoa_buffer_bytes(unsigned C) {
-    return (size_t(16) + sizeof(typename QaoaCostWord<CostT>::type)) * qaoa_padded(C);
+    const size_t b = (size_t(16) + sizeof(typename QaoaCostWord<CostT>::type)) * qaoa_padded(C);
+    return (b + 127) & ~size_t(127);
+}
+
+// Alignment of every region of a block's shared memory (base aligned to 128 bytes): the
+// 16-byte amplitudes and the asynchronous copies into them, the cost words, the doubles of
+// the reduction.
+template <class CostT>
+ORKAN_HD bool qaoa_smem_aligned(unsigned C, unsigned ring) {
+    const size_t w = sizeof(typename QaoaCostWord<CostT>::type);
+    for (unsigned slot = 0; slot < ring; ++slot) {
+        const size_t vb = qaoa_buffer_bytes<CostT>(C) * slot, cw = vb + size_t(16) * qaoa_padded(C);
+        if (vb % 16 || cw % w) return false;
+    }
+    return (qaoa_buffer_bytes<CostT>(C) * ring) % 8 == 0;
 }
 template <class CostT>
 ORKAN_HD size_t qaoa_smem_bytes(unsigned C, unsigned nthr, unsigned ring) {

@@ -381,6 +381,15 @@ int emu_fill(double* data, uint64_t len, double re, double im, unsigned corner_l
     return 0;
 }
 
+// Shared-memory layout of the QAOA pass kernel: 1 when every region is aligned for all
+// chunk sizes 0..13 and ring depths 1, 2, for both cost types.
+int emu_qaoa_smem_aligned(void) {
+    for (unsigned C = 0; C <= kQaoaMaxC; ++C)
+        for (unsigned ring = 1; ring <= 2; ++ring)
+            if (!qaoa_smem_aligned<uint8_t>(C, ring) || !qaoa_smem_aligned<double>(C, ring)) return 0;
+    return 1;
+}
+
 // Fused QAOA passes of one instance; byte_cost selects byte costs (cost_b) over doubles.
 int emu_qaoa(unsigned n, const double* cost_d, const uint8_t* cost_b, int byte_cost, unsigned p, const double* gamma,
              const double* beta, unsigned C, unsigned nthr, unsigned upto, double* psi, double* mean,

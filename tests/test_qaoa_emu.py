@@ -123,3 +123,10 @@ def test_mixer_forms_and_edge_angles(n, C):
     res, m = kemu.qaoa(n, cost, 5, g, b, log_chunk=C, nthr=32, byte_cost=True)
     assert res.oob == 0
     assert abs(m - R.qaoa_mean(n, cost, g, b)) < 1e-12
+
+
+def test_shared_memory_regions_aligned_for_every_chunk():
+    """Amplitude slots (16-byte asynchronous copies), cost words and the reduction array
+    stay aligned for every chunk size and buffer depth (a misaligned region faults on the
+    GPU, not on the CPU emulator)."""
+    assert kemu.lib().emu_qaoa_smem_aligned() == 1
