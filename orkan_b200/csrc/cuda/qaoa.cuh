@@ -126,6 +126,21 @@ ORKAN_HD unsigned qaoa_bit(unsigned n, unsigned C, unsigned kind, unsigned q) {
     return kind == kQaoaHigh ? q - C : q;
 }
 
+// Slot of position r of a high chunk's enumeration with the K slot bits at B0 left out
+// (K = 0: every slot).  Lanes 0-7 take the lowest free row bits, so the 8 lanes of a
+// shared-memory phase hit consecutive slots; the next two lane bits take column bits, so a
+// warp reads or writes runs of up to 4 neighbouring amplitudes (64 bytes) of 8 rows; the
+// rest takes the other free row bits, then the other column bits.
+ORKAN_HD unsigned qaoa_high_slot(unsigned r, unsigned R, unsigned lw, unsigned B0, unsigned K) {
+    const unsigned nr = R - K;                       // free row bits
+    const unsigned a = nr < 3 ? nr : 3, c = lw < 2 ? lw : 2;
+    const unsigned rest = r >> (a + c);
+    const unsigned rr = (r & ((1u << a) - 1)) | ((rest & ((1u << (nr - a)) - 1)) << a);
+    const unsigned col = ((r >> a) & ((1u << c) - 1)) | ((rest >> (nr - a)) << c);
+    const unsigned row = (rr & ((1u << B0) - 1)) | ((rr >> B0) << (B0 + K));
+    return row | (col << R);
+}
+
 // Work item w -> position in the pass's instance list (binary search over item0).
 ORKAN_HD unsigned qaoa_find(const QaoaInst* inst, unsigned ninst, idx_t w) {
     unsigned lo = 0, hi = ninst;
@@ -303,7 +318,9 @@ template <class CostT, class Mem, class CostMem>
 ORKAN_HD void qaoa_fill(const QaoaPass& P, const QaoaInst& I, const QaoaPlan& pl, const Mem& psi, const CostMem& cost,
                         idx_t chunk, const QaoaSmem<CostT>& S, unsigned tid, unsigned nthr) {
     const unsigned cnt = 1u << qaoa_lc(I.n, P.C, P.kind);
-    for (unsigned s = tid; s < cnt; s += nthr) {
+    const unsigned R = I.n - P.C, lw = P.kind == kQaoaHigh ? qaoa_logw(I.n, P.C) : 0u;
+    for (unsigned e = tid; e < cnt; e += nthr) {
+        const unsigned s = P.kind == kQaoaHigh ? qaoa_high_slot(e, R, lw, 0, 0) : e;
         const idx_t x = qaoa_index(I.n, P.C, P.kind, chunk, s);
         if (!pl.init) psi.cp16(S.vb + qaoa_pad(s), x);
         cost.cpw(S.cw + qaoa_pad(s), x);
@@ -331,8 +348,10 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
     const idx_t row = (idx_t)I.pos * P.p;
     const double amp0 = 1.0 / sqrt((double)(idx_t(1) << n));
     double acc = 0.0;
+    const bool high = P.kind == kQaoaHigh;
+    const unsigned R = high ? n - P.C : 0u, lw = high ? qaoa_logw(n, P.C) : 0u;
     for (unsigned r = tid; r < sets; r += nthr) {
-        const unsigned base = (r & LOWM) | ((r >> B0) << (B0 + K));
+        const unsigned base = high ? qaoa_high_slot(r, R, lw, B0, K) : (r & LOWM) | ((r >> B0) << (B0 + K));
         const unsigned p0 = qaoa_pad(base);
         const idx_t xb = qaoa_index(n, P.C, P.kind, chunk, base);      // slot base | j << B0 is xb + j xs
         // cost of element j, read from the staged words where it is used
