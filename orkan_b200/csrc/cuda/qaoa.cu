@@ -52,10 +52,10 @@ __global__ void k_qaoa_tables(const unsigned* cmax, const double* gamma, unsigne
 template <unsigned NT, class CostT, unsigned RING>
 __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_qaoa_pass(QaoaPass P, QaoaTables T) {
     extern __shared__ __align__(16) unsigned char smem_q[];
-    const unsigned lc = P.kind == kQaoaFull ? P.inst[0].n : P.C;
+    const unsigned lc = P.kind == kQaoaFull ? P.plan.q1 : P.C;
     auto fill = [&](idx_t w, unsigned slot) {
         const QaoaInst I = P.inst[qaoa_find(P.inst, P.ninst, w)];
-        const QaoaPlan pl = qaoa_plan(I.n, P.C, P.kind, P.p, P.pass);
+        const QaoaPlan& pl = P.plan;
         const QaoaSmem<CostT> S = qaoa_smem_at<CostT>(smem_q, lc, NT, RING, slot);
         qaoa_fill<CostT>(P, I, pl, QaoaDevPsi{I.psi}, QaoaDevCost<CostT>{static_cast<const CostT*>(I.cost)},
                          w - I.item0, S, threadIdx.x, NT);
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_qaoa_pass(QaoaPass P
         }
         __syncthreads();
         const QaoaInst I = P.inst[qaoa_find(P.inst, P.ninst, w)];
-        const QaoaPlan pl = qaoa_plan(I.n, P.C, P.kind, P.p, P.pass);
+        const QaoaPlan& pl = P.plan;
         const QaoaSmem<CostT> S = qaoa_smem_at<CostT>(smem_q, lc, NT, RING, slot);
         const unsigned nst = qaoa_stages(pl);
         for (unsigned st = 0; st < nst; ++st) {
@@ -179,6 +179,7 @@ struct Launch {
     unsigned inst_off, ninst;      // slice of the plan's instance records
     idx_t items;
     unsigned pass, C, kind, nt, ring;
+    unsigned n;                    // qubit count of every instance of the launch
     unsigned grid;                 // blocks (pass launches)
     bool bytes;                    // byte costs
     size_t partial_off;
@@ -283,6 +284,7 @@ Plan make_plan(const orkan_qaoa* b, const std::vector<unsigned>& sel) {
                     L.C = C;
                     L.kind = full ? kQaoaFull : ((j % 2 == 0) ? kQaoaLow : kQaoaHigh);
                     L.nt = b->cfg[nq].nt;
+                    L.n = nq;
                     L.ring = b->cfg[nq].ring;
                     L.bytes = bytes_cost;
                     idx_t acc = 0;
@@ -366,6 +368,7 @@ int enqueue_kernels(const orkan_qaoa* b, const Plan& pl, cudaStream_t st) {
             P.pass = L.pass;
             P.C = L.C;
             P.kind = L.kind;
+            qaoa_pass_setup(P, L.n);
             rc = L.bytes ? launch_pass_t<uint8_t>(L.nt, L.ring, L.C, L.grid, P, T, st)
                          : launch_pass_t<double>(L.nt, L.ring, L.C, L.grid, P, T, st);
         } else {
@@ -426,8 +429,9 @@ void stage_angles(orkan_qaoa* b, const double* gammas, const double* betas) {
     const size_t np = (size_t)b->count * b->p;
     for (size_t k = 0; k < np; ++k) {
         const double theta = 2.0 * betas[k];
+        const unsigned n = b->n[k / b->p];
         b->h_gamma[k] = gammas[k];
-        b->h_rx[k] = qaoa_rx_coeffs(cos(theta / 2.0), sin(theta / 2.0));
+        b->h_rx[k] = qaoa_rx_coeffs(cos(theta / 2.0), sin(theta / 2.0), n, b->cfg[n].C);
     }
 }
 

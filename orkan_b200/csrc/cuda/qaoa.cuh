@@ -59,32 +59,29 @@ struct QaoaInst {
     unsigned pos;          // row of the instance in the angle arrays and tables
 };
 
-struct QaoaPass {
-    const QaoaInst* inst;
-    unsigned ninst;
-    idx_t items;           // total work items of the pass
-    const double* gamma;   // [pos][p]
-    double* partial;       // measuring pass: one partial sum per work item
-    unsigned p;
-    unsigned pass;         // j in [0, p] (0 for full passes)
-    unsigned C;            // log2 of the chunk (amplitudes per item)
-    unsigned kind;         // QaoaKind
-};
-
-// The mixer of one layer in the four-FMA form: k, the dropped factor, and which form.
+// The mixer of one layer of one instance in the four-FMA form: k, which form, and the
+// product of the dropped factors over the qubits a segment mixes, by pass kind
+// (f[kind]: n qubits for a full pass, C for a low one, n - C for a high one).
 struct QaoaRx {
     double k;
-    double scale;
+    double f[3];
     int sform;             // 0: (a - i k b) with k = s / c, scale = c; 1: (k a - i b), k = c / s, scale = s
     int pad_;
 };
 
 // Host side: the mixer coefficients of rx(theta) = exp(-i theta X / 2) from c = cos(theta / 2),
-// s = sin(theta / 2).
-inline QaoaRx qaoa_rx_coeffs(double c, double s) {
+// s = sin(theta / 2), for an instance of n qubits in chunks of 2^C.
+inline QaoaRx qaoa_rx_coeffs(double c, double s, unsigned n, unsigned C) {
     QaoaRx r;
-    if (fabs(c) >= fabs(s)) { r.k = s / c; r.scale = c; r.sform = 0; }
-    else { r.k = c / s; r.scale = s; r.sform = 1; }
+    double scale;
+    if (fabs(c) >= fabs(s)) { r.k = s / c; scale = c; r.sform = 0; }
+    else { r.k = c / s; scale = s; r.sform = 1; }
+    const unsigned nq[3] = {n, C < n ? C : n, C < n ? n - C : 0u};
+    for (unsigned kd = 0; kd < 3; ++kd) {
+        double f = 1.0;
+        for (unsigned i = 0; i < nq[kd]; ++i) f *= scale;
+        r.f[kd] = f;
+    }
     r.pad_ = 0;
     return r;
 }
@@ -214,32 +211,62 @@ enum : unsigned { kQaoaFromSmem = 0, kQaoaFromGlobal = 1, kQaoaFromInit = 2 };
 enum : unsigned { kQaoaToSmem = 0, kQaoaToGlobal = 1, kQaoaToMeasure = 2 };
 
 struct QaoaStage {
-    unsigned g;                // group
-    unsigned t0, t1;           // segments applied in this stage
-    unsigned src, dst;
-    int pre_phase;             // phase of segment t0's preceding layer applied before it (-1: none)
-    int end0;                  // segment t0 ends in this stage (all of t0..t1 when there is one group)
+    uint8_t g;                 // group
+    uint8_t t0, t1;            // segments applied in this stage
+    uint8_t src, dst;
+    int8_t pre_phase;          // phase of segment t0's preceding layer applied before it (-1: none)
+    uint8_t end0;              // segment t0 ends in this stage (all of t0..t1 when there is one group)
+    uint8_t pad_;
 };
 
 // Register stage r of a pass.  Stages 0..m-1 run segment 0's groups; every later segment
 // adds m - 1 stages (its first group shares the previous segment's last stage).
 ORKAN_HD QaoaStage qaoa_reg_stage(const QaoaPlan& pl, unsigned r) {
     QaoaStage s;
+    s.pad_ = 0;
     if (pl.m == 1) {
-        s.g = 0; s.t0 = 0; s.t1 = pl.segs - 1; s.end0 = 1;
+        s.g = 0; s.t0 = 0; s.t1 = (uint8_t)(pl.segs - 1); s.end0 = 1;
     } else {
         unsigned t, i;
         if (r < pl.m) { t = 0; i = r; }
         else { const unsigned k = r - pl.m; t = 1 + k / (pl.m - 1); i = 1 + k % (pl.m - 1); }
-        s.g = qaoa_order(pl, t, i);
-        s.t0 = t;
-        s.t1 = (i == pl.m - 1 && t + 1 < pl.segs) ? t + 1 : t;
+        s.g = (uint8_t)qaoa_order(pl, t, i);
+        s.t0 = (uint8_t)t;
+        s.t1 = (uint8_t)((i == pl.m - 1 && t + 1 < pl.segs) ? t + 1 : t);
         s.end0 = i == pl.m - 1;
     }
     s.src = (r == 0 && pl.init) ? kQaoaFromInit : kQaoaFromSmem;
     s.dst = r + 1 == pl.nreg ? (pl.measure ? kQaoaToMeasure : kQaoaToGlobal) : kQaoaToSmem;
-    s.pre_phase = (r == 0) ? pl.phase_load : -1;
+    s.pre_phase = (int8_t)((r == 0) ? pl.phase_load : -1);
     return s;
+}
+
+// A pass launch: its instances (all of one qubit count), the pass's plan and, when they
+// fit, its register stages, computed once on the host.
+constexpr unsigned kQaoaStageTable = 16;
+
+struct QaoaPass {
+    const QaoaInst* inst;
+    unsigned ninst;
+    idx_t items;           // total work items of the pass
+    const double* gamma;   // [pos][p]
+    double* partial;       // measuring pass: one partial sum per work item
+    unsigned p;
+    unsigned pass;         // j in [0, p] (0 for full passes)
+    unsigned C;            // log2 of the chunk (amplitudes per item)
+    unsigned kind;         // QaoaKind
+    QaoaPlan plan;         // qaoa_plan(n, C, kind, p, pass) of the launch's qubit count
+    QaoaStage stage[kQaoaStageTable];   // qaoa_reg_stage(plan, r) for r < nreg <= kQaoaStageTable
+};
+
+// Fill in the plan and the stage table of a pass of n-qubit instances.
+ORKAN_HD void qaoa_pass_setup(QaoaPass& P, unsigned n) {
+    P.plan = qaoa_plan(n, P.C, P.kind, P.p, P.pass);
+    for (unsigned r = 0; r < kQaoaStageTable; ++r)
+        P.stage[r] = r < P.plan.nreg ? qaoa_reg_stage(P.plan, r) : QaoaStage{};
+}
+ORKAN_HD QaoaStage qaoa_stage_desc(const QaoaPass& P, unsigned r) {
+    return P.plan.nreg <= kQaoaStageTable ? P.stage[r] : qaoa_reg_stage(P.plan, r);
 }
 
 ORKAN_HD double2 qaoa_apply_phase(double2 ph, double2 v) {
@@ -318,19 +345,21 @@ template <class CostT, class Mem, class CostMem>
 ORKAN_HD void qaoa_fill(const QaoaPass& P, const QaoaInst& I, const QaoaPlan& pl, const Mem& psi, const CostMem& cost,
                         idx_t chunk, const QaoaSmem<CostT>& S, unsigned tid, unsigned nthr) {
     const unsigned cnt = 1u << qaoa_lc(I.n, P.C, P.kind);
-    const unsigned R = I.n - P.C, lw = P.kind == kQaoaHigh ? qaoa_logw(I.n, P.C) : 0u;
+    if (P.kind != kQaoaHigh) {                     // contiguous chunk: equally spaced copies
+        const idx_t x0 = P.kind == kQaoaLow ? chunk << P.C : 0;
+        for (unsigned e = tid; e < cnt; e += nthr) {
+            if (!pl.init) psi.cp16(S.vb + qaoa_pad(e), x0 + e);
+            cost.cpw(S.cw + qaoa_pad(e), x0 + e);
+        }
+        return;
+    }
+    const unsigned R = I.n - P.C, lw = qaoa_logw(I.n, P.C);
     for (unsigned e = tid; e < cnt; e += nthr) {
-        const unsigned s = P.kind == kQaoaHigh ? qaoa_high_slot(e, R, lw, 0, 0) : e;
+        const unsigned s = qaoa_high_slot(e, R, lw, 0, 0);
         const idx_t x = qaoa_index(I.n, P.C, P.kind, chunk, s);
         if (!pl.init) psi.cp16(S.vb + qaoa_pad(s), x);
         cost.cpw(S.cw + qaoa_pad(s), x);
     }
-}
-
-ORKAN_HD double qaoa_powu(double x, unsigned e) {
-    double r = 1.0;
-    for (unsigned i = 0; i < e; ++i) r *= x;
-    return r;
 }
 
 // Register stage of a group of K slot bits starting at B0 (0, 4, 8 or 12).
@@ -344,9 +373,9 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
     const unsigned n = I.n;
     const unsigned sets = 1u << (lc - K);
     const idx_t xs = qaoa_stride(n, P.C, P.kind, B0);
-    const unsigned nq = pl.q1 - pl.q0;
     const idx_t row = (idx_t)I.pos * P.p;
     const double amp0 = 1.0 / sqrt((double)(idx_t(1) << n));
+    const unsigned x3s = (unsigned)xs & 3u;
     double acc = 0.0;
     const bool high = P.kind == kQaoaHigh;
     const unsigned R = high ? n - P.C : 0u, lw = high ? qaoa_logw(n, P.C) : 0u;
@@ -354,12 +383,16 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
         const unsigned base = high ? qaoa_high_slot(r, R, lw, B0, K) : (r & LOWM) | ((r >> B0) << (B0 + K));
         const unsigned p0 = qaoa_pad(base);
         const idx_t xb = qaoa_index(n, P.C, P.kind, chunk, base);      // slot base | j << B0 is xb + j xs
+        const unsigned x3 = (unsigned)xb & 3u;
         // cost of element j, read from the staged words where it is used
         auto cost_of = [&](unsigned j) -> CostT {
             if constexpr (std::is_same<CostT, double>::value) {
                 return S.cw[p0 + j * D];
             } else {
-                return (CostT)((S.cw[p0 + j * D] >> (8u * ((unsigned)(xb + j * xs) & 3u))) & 0xffu);
+                // byte of amplitude xb + j xs in its word: j moves it only when the group
+                // starts at slot bit 0 of a contiguous chunk (xs = 1)
+                const unsigned sh = (B0 == 0 && x3s) ? 8u * ((x3 + j) & 3u) : 8u * x3;
+                return (CostT)((S.cw[p0 + j * D] >> sh) & 0xffu);
             }
         };
         double2 v[NV];
@@ -379,7 +412,7 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
         }
         for (unsigned t = sg.t0; t <= sg.t1; ++t) {
             const unsigned layer = pl.layer0 + t;
-            const QaoaRx rx = T.rx[row + layer];
+            const QaoaRx& rx = T.rx[row + layer];
             const double k = rx.k;
             if (rx.sform == 0) {
 #pragma unroll
@@ -408,7 +441,7 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
             }
             const bool ends = (pl.m == 1) || (t == sg.t0 && sg.end0);
             if (t < sg.t1) {                                  // scale of segment t, phase of the next layer
-                const double f = qaoa_powu(rx.scale, nq);
+                const double f = rx.f[P.kind];
                 const double gam = P.gamma[row + layer + 1];
                 const double2* tb = T.phase + (row + layer + 1) * T.tstride;
 #pragma unroll
@@ -417,7 +450,7 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
                     v[j] = qaoa_apply_phase(c2(ph.x * f, ph.y * f), v[j]);
                 }
             } else if (ends) {
-                const double f = qaoa_powu(rx.scale, nq);
+                const double f = rx.f[P.kind];
 #pragma unroll
                 for (unsigned j = 0; j < NV; ++j) v[j] = c2(v[j].x * f, v[j].y * f);
             }
@@ -444,7 +477,7 @@ ORKAN_HD void qaoa_stage(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
                          unsigned nthr) {
     const unsigned n = I.n, kind = P.kind;
     if (st < pl.nreg) {
-        const QaoaStage sg = qaoa_reg_stage(pl, st);
+        const QaoaStage sg = qaoa_stage_desc(P, st);
         const unsigned lc = qaoa_lc(n, P.C, kind);
         const unsigned nq = pl.q1 - pl.q0;
         const unsigned off = sg.g * kQaoaGroup;

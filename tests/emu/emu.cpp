@@ -177,7 +177,8 @@ int run_qaoa(unsigned n, const CostT* cost, unsigned p, const double* gamma, con
     std::vector<QaoaRx> rx(p);
     std::vector<double2> table(1, c2(1.0, 0.0));
     unsigned tstride = 1;
-    for (unsigned k = 0; k < p; ++k) rx[k] = qaoa_rx_coeffs(cos(2.0 * beta[k] / 2.0), sin(2.0 * beta[k] / 2.0));
+    for (unsigned k = 0; k < p; ++k)
+        rx[k] = qaoa_rx_coeffs(cos(2.0 * beta[k] / 2.0), sin(2.0 * beta[k] / 2.0), n, C);
     if (sizeof(CostT) == 1) {
         unsigned cmax = 0;
         for (idx_t x = 0; x < dim; ++x) cmax = cost[x] > cmax ? (unsigned)cost[x] : cmax;
@@ -212,8 +213,9 @@ int run_qaoa(unsigned n, const CostT* cost, unsigned p, const double* gamma, con
         P.partial = partial.data();
         P.p = p;
         P.pass = full ? 0 : j;
+        qaoa_pass_setup(P, n);
         const QaoaTables T{table.data(), rx.data(), tstride};
-        const QaoaPlan pl = qaoa_plan(n, P.C, P.kind, p, P.pass);
+        const QaoaPlan& pl = P.plan;
         std::vector<unsigned char> smem(qaoa_smem_bytes<CostT>(P.C, nthr, 1));
         const QaoaSmem<CostT> S = qaoa_smem_at<CostT>(smem.data(), P.C, nthr, 1, 0);
         for (idx_t w = 0; w < P.items; ++w) {
