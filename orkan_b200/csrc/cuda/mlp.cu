@@ -7,6 +7,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <vector>
@@ -15,7 +16,7 @@ namespace {
 
 std::atomic<unsigned long long> g_launches{0};
 
-constexpr int kBM = 64, kBN = 64, kBK = 16, kGemmThreads = 256;
+constexpr int kBM = 64, kBN = 64, kBK = 16, kGemmThreads = 256;   // default tile; 32 x 32 for small grids
 constexpr float kInvSqrt2 = 0.70710678118654752440f;
 constexpr float kInvSqrt2Pi = 0.39894228040143267794f;
 
@@ -30,54 +31,60 @@ enum Epi : int { kEpiStore = 0, kEpiBiasGelu = 1, kEpiGeluBack = 2 };
 // opB[k][n] = TB ? B[n][k] : B[k][n] (row-major with leading dimensions lda, ldb).
 // Epilogues: store; z = acc + bias[n] into C and gelu(z) into out2; acc * gelu'(aux[m][n]).
 // Each output is one thread's fixed-order sum over k, so results are deterministic.
-template <bool TA, bool TB, int EPI>
+template <bool TA, bool TB, int EPI, int kBM = 64, int kBN = 64>
 __global__ void __launch_bounds__(kGemmThreads) k_gemm(int M, int N, int K, const float* __restrict__ A, int lda,
                                                        const float* __restrict__ B, int ldb, float* __restrict__ C,
                                                        int ldc, const float* __restrict__ bias,
                                                        const float* __restrict__ aux, float* __restrict__ out2) {
+    constexpr int TM = kBM / 16, TN = kBN / 16;          // outputs per thread: TM x TN
     __shared__ float As[kBK][kBM + 4];
     __shared__ float Bs[kBK][kBN + 4];
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
-    float acc[4][4];
+    // split over k (gridDim.z slices of whole kBK tiles): slice z sums its own k range and
+    // stores to its own M x ldc plane of C
+    const int ktiles = (K + kBK - 1) / kBK, per = (ktiles + gridDim.z - 1) / gridDim.z;
+    const int kbeg = blockIdx.z * per * kBK, kend = min(K, (int)(blockIdx.z + 1) * per * kBK);
+    C += (size_t)blockIdx.z * M * ldc;
+    float acc[TM][TN];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
-    for (int k0 = 0; k0 < K; k0 += kBK) {
+        for (int j = 0; j < TN; ++j) acc[i][j] = 0.f;
+    for (int k0 = kbeg; k0 < kend; k0 += kBK) {
         for (int e = threadIdx.x; e < kBM * kBK; e += kGemmThreads) {
             const int mm = TA ? e % kBM : e / kBK, kk = TA ? e / kBM : e % kBK;
             const int gm = m0 + mm, gk = k0 + kk;
             float v = 0.f;
-            if (gm < M && gk < K) v = TA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk];
+            if (gm < M && gk < kend) v = TA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk];
             As[kk][mm] = v;
         }
         for (int e = threadIdx.x; e < kBN * kBK; e += kGemmThreads) {
             const int nn = TB ? e / kBK : e % kBN, kk = TB ? e % kBK : e / kBN;
             const int gn = n0 + nn, gk = k0 + kk;
             float v = 0.f;
-            if (gn < N && gk < K) v = TB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn];
+            if (gn < N && gk < kend) v = TB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn];
             Bs[kk][nn] = v;
         }
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < kBK; ++kk) {
-            float a[4], b[4];
+            float a[TM], b[TN];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+            for (int i = 0; i < TM; ++i) a[i] = As[kk][ty + 16 * i];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+            for (int j = 0; j < TN; ++j) b[j] = Bs[kk][tx + 16 * j];
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < TM; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < TN; ++j) {
             const int m = m0 + ty + 16 * i, n = n0 + tx + 16 * j;
             if (m >= M || n >= N) continue;
             const size_t o = (size_t)m * ldc + n;
@@ -91,6 +98,15 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(int M, int N, int K, cons
                 C[o] = acc[i][j] * gelu_grad(aux[o]);
             }
         }
+}
+
+// out[i] = sum over the slices z < nz of part[z * count + i], in slice order.
+__global__ void k_sum_slices(const float* __restrict__ part, int nz, size_t count, float* __restrict__ out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    float s = 0.f;
+    for (int z = 0; z < nz; ++z) s += part[(size_t)z * count + i];
+    out[i] = s;
 }
 
 // y[b] = sum_h A[b][h] w[h] + w0, one warp per row, fixed shuffle tree.
@@ -244,6 +260,8 @@ struct orkan_mlp {
     float *P = nullptr, *G = nullptr, *M1 = nullptr, *M2 = nullptr;
     float *Z1 = nullptr, *A1 = nullptr, *Z2 = nullptr, *A2 = nullptr, *y = nullptr, *dy = nullptr;
     float *dZ2 = nullptr, *dZ1 = nullptr, *xb = nullptr, *tb = nullptr, *loss = nullptr, *losses = nullptr;
+    float* split = nullptr;             // k-slice partial products of the weight gradients
+    size_t split_cap = 0;
     unsigned* step = nullptr;
     size_t losses_cap = 0;
 };
@@ -254,8 +272,32 @@ template <bool TA, bool TB, int EPI>
 void gemm(cudaStream_t st, int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C, int ldc,
           const float* bias = nullptr, const float* aux = nullptr, float* out2 = nullptr) {
     const dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
-    k_gemm<TA, TB, EPI><<<grid, kGemmThreads, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc, bias, aux, out2);
+    if (grid.x * grid.y >= 148) {
+        k_gemm<TA, TB, EPI><<<grid, kGemmThreads, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc, bias, aux, out2);
+    } else {                                   // 32 x 32 tiles: four times the blocks
+        const dim3 g2((N + 31) / 32, (M + 31) / 32);
+        k_gemm<TA, TB, EPI, 32, 32><<<g2, kGemmThreads, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc, bias, aux, out2);
+    }
     ++g_launches;
+}
+
+// C[M][N] (ldc = N) = sum over a long k (the batch) of A^T B, split into k slices so that
+// the grid covers the SMs; the slices are summed in order (deterministic).
+void gemm_tn_split(orkan_mlp* m, cudaStream_t st, int M, int N, int K, const float* A, int lda, const float* B,
+                   int ldb, float* C) {
+    const int tiles = ((N + kBN - 1) / kBN) * ((M + kBM - 1) / kBM);
+    int nz = (296 + tiles - 1) / tiles;
+    nz = std::max(1, std::min(nz, (K + kBK - 1) / kBK));
+    if (nz == 1 || (size_t)nz * M * N > m->split_cap) {
+        gemm<true, false, kEpiStore>(st, M, N, K, A, lda, B, ldb, C, N);
+        return;
+    }
+    const dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM, nz);
+    k_gemm<true, false, kEpiStore><<<grid, kGemmThreads, 0, st>>>(M, N, K, A, lda, B, ldb, m->split, N, nullptr,
+                                                                  nullptr, nullptr);
+    const size_t cnt = (size_t)M * N;
+    k_sum_slices<<<blocks(cnt, 256), 256, 0, st>>>(m->split, nz, cnt, C);
+    g_launches += 2;
 }
 
 // Forward of `batch` rows of x into m->Z1, A1, Z2, A2, y.
@@ -275,11 +317,11 @@ void backward(orkan_mlp* m, const float* x, int batch, float* g, float* gx, cuda
     k_colsum<<<1, 32, 0, st>>>(m->dy, batch, 1, g + m->ob3);
     k_outer_gelu<<<blocks((size_t)batch * H, 256), 256, 0, st>>>(m->dy, m->P + m->oW3, m->Z2, batch, H, m->dZ2);
     g_launches += 3;
-    gemm<true, false, kEpiStore>(st, H, H, batch, m->A1, H, m->dZ2, H, g + m->oW2, H);
+    gemm_tn_split(m, st, H, H, batch, m->A1, H, m->dZ2, H, g + m->oW2);
     k_colsum<<<blocks(H, 128), 128, 0, st>>>(m->dZ2, batch, H, g + m->ob2);
     ++g_launches;
     gemm<false, true, kEpiGeluBack>(st, batch, H, H, m->dZ2, H, m->P + m->oW2, H, m->dZ1, H, nullptr, m->Z1);
-    gemm<true, false, kEpiStore>(st, I, H, batch, x, I, m->dZ1, H, g + m->oW1, H);
+    gemm_tn_split(m, st, I, H, batch, x, I, m->dZ1, H, g + m->oW1);
     k_colsum<<<blocks(H, 128), 128, 0, st>>>(m->dZ1, batch, H, g + m->ob1);
     ++g_launches;
     if (gx) gemm<false, true, kEpiStore>(st, batch, I, H, m->dZ1, H, m->P + m->oW1, H, gx, I);
@@ -340,6 +382,8 @@ int orkan_mlp_create(orkan_mlp_t** out, unsigned n_in, unsigned hidden, unsigned
     al(&m->xb, B * I);
     al(&m->tb, B);
     al(&m->loss, 1);
+    m->split_cap = (size_t)32 * std::max(I, H) * H;
+    al(&m->split, m->split_cap);
     if (!rc) rc = (int)cudaMalloc(reinterpret_cast<void**>(&m->step), 2 * sizeof(unsigned));
     if (rc) {
         orkan_mlp_destroy(m);
@@ -369,7 +413,7 @@ int orkan_mlp_create(orkan_mlp_t** out, unsigned n_in, unsigned hidden, unsigned
 void orkan_mlp_destroy(orkan_mlp_t* m) {
     if (!m) return;
     float* bufs[] = {m->P, m->G, m->M1, m->M2, m->Z1, m->A1, m->Z2, m->A2, m->dZ2, m->dZ1,
-                     m->y, m->dy, m->xb, m->tb, m->loss, m->losses};
+                     m->y, m->dy, m->xb, m->tb, m->loss, m->losses, m->split};
     for (float* b : bufs) cudaFree(b);
     cudaFree(m->step);
     delete m;
