@@ -56,6 +56,21 @@ def parse_args():
     return ap.parse_args()
 
 
+def reduce_max(x: float, dist, device) -> float:
+    """The maximum of x over all ranks of the process group (x itself without one)."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world: int, steps: int, bytes_per_step: float, max_ms: float) -> float:
+    """Whole-job GB/s of N replicas: every rank's bytes over the slowest rank's time."""
+    return world * steps * bytes_per_step / (max_ms * 1e-3) / 1e9
+
+
 def host_cores() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -497,11 +512,7 @@ def run_gpu(args):
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, "cuda")
 
     ork = orkan_b200.load(5)
     ork.set_stream(torch.cuda.current_stream().cuda_stream)
@@ -569,7 +580,7 @@ def run_gpu(args):
             per_class_bytes[cls] = per_class_bytes.get(cls, 0) + e[5]
             per_class_n[cls] = per_class_n.get(cls, 0) + 1
     max_ms = max_over_ranks(total_ms)
-    value = world * args.steps * step_bytes / (max_ms * 1e-3) / 1e9
+    value = replica_value(world, args.steps, step_bytes, max_ms)
 
     # ---- end to end through the public API with host buffers ----
     e2e = None
