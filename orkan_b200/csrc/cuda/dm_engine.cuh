@@ -40,7 +40,8 @@ struct DmGeom {
     idx_t d;            // 2^n
     unsigned n;
     unsigned ls;        // log2 of the sub-tile side S
-    unsigned h;         // gate qubits with position >= ls
+    unsigned h;         // pairing bits: the gate qubits with position >= ls, or qubit ls alone
+                        // when every gate qubit lies inside the sub-tile
     unsigned hb[3];     // their positions in segment-index space (q - ls), ascending
     unsigned k;         // gate qubits
     unsigned vbit[3];   // virtual-index bit of gate qubit j; j = 0 is the MSB of the local index
@@ -72,14 +73,19 @@ inline bool dm_geometry(unsigned n, unsigned k, const unsigned* qubits, unsigned
         for (unsigned j = 0; j < k; ++j) h += (qubits[j] >= ls);
         const unsigned long long cap = h <= 1 ? (unsigned long long)max_v_low * max_v_low : kDmMaxElems;
         if ((1ull << (2 * (ls + h))) <= cap || ls == 0) {
+            // a gate that stays inside the sub-tile (h = 0) still pairs the sub-tiles along
+            // qubit ls when the doubled block fits: four times fewer, four times larger items
+            const bool widen = (h == 0 && ls < n && (1ull << (2 * (ls + 1))) <= cap);
             g->d = idx_t(1) << n;
             g->n = n;
             g->ls = ls;
-            g->h = h;
+            g->h = widen ? 1u : h;
             g->k = k;
             // high qubits in ascending order -> hb, and their virtual bits ls + rank
             unsigned hq[3], nh = 0;
             for (unsigned j = 0; j < k; ++j) if (qubits[j] >= ls) hq[nh++] = qubits[j];
+            if (widen) hq[nh++] = ls;
+            h = g->h;
             for (unsigned a = 0; a < nh; ++a)
                 for (unsigned b = a + 1; b < nh; ++b)
                     if (hq[b] < hq[a]) { unsigned t = hq[a]; hq[a] = hq[b]; hq[b] = t; }
