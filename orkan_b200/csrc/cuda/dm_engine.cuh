@@ -476,24 +476,27 @@ struct OpSuper1 {
 // Monomial gate U|x> with an involutive permutation (X, Y, CX, CY, SWAP, CCX ...):
 // (U psi)[y] = phase[y] * psi[src[y]] on the local index, src[src[y]] == y.
 // Element pairs (y, z) <-> (src y, src z) are 2-cycles; the thread owning the
-// smaller flat index of a pair updates both.
+// smaller flat index of a pair updates both.  The permutation and the phases are looked up
+// per virtual index (tables sig / vph of the block, filled once per launch by
+// dm_monomial_tables) instead of being assembled from the gate bits per element.
 struct OpMonomial {
     unsigned src[8];
     double2 phase[8];
+    unsigned char sig[kDmMaxV];   // virtual index -> virtual index of its image
+    double2 vph[kDmMaxV];         // phase of the local index of virtual index x
     ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
-        const unsigned V = g.V(), P = g.P(), k = g.k, lv = g.ls + g.h;
+        const unsigned V = g.V(), P = g.P(), lv = g.ls + g.h;
         const unsigned total = V * V;
         for (unsigned f = tid; f < total; f += nthr) {
             const unsigned r = f >> lv, c = f & (V - 1);
-            const unsigned lr = dm_get_local(r, g.vbit, k), lc = dm_get_local(c, g.vbit, k);
-            const unsigned r2 = dm_set_local(r, src[lr], g.vbit, k), c2i = dm_set_local(c, src[lc], g.vbit, k);
+            const unsigned r2 = sig[r], c2i = sig[c];
             const unsigned f2 = (r2 << lv) + c2i;
             if (f2 < f) continue;
-            const double2 fa = cmulc(phase[lr], phase[lc]);
+            const double2 fa = cmulc(vph[r], vph[c]);
             if (f2 == f) {
                 vb[r * P + c] = cmul(fa, vb[r * P + c]);
             } else {
-                const double2 fb = cmulc(phase[src[lr]], phase[src[lc]]);
+                const double2 fb = cmulc(vph[r2], vph[c2i]);
                 const double2 va = vb[r * P + c], vb2 = vb[r2 * P + c2i];
                 vb[r * P + c] = cmul(fa, vb2);
                 vb[r2 * P + c2i] = cmul(fb, va);
@@ -501,6 +504,20 @@ struct OpMonomial {
         }
     }
 };
+
+// Per-virtual-index tables of a monomial gate for the geometry g.
+inline void dm_monomial_tables(OpMonomial& op, const DmGeom& g) {
+    for (unsigned x = 0; x < kDmMaxV; ++x) {
+        if (x < g.V()) {
+            const unsigned l = dm_get_local(x, g.vbit, g.k);
+            op.sig[x] = (unsigned char)dm_set_local(x, op.src[l], g.vbit, g.k);
+            op.vph[x] = op.phase[l];
+        } else {
+            op.sig[x] = (unsigned char)x;
+            op.vph[x] = c2(1.0, 0.0);
+        }
+    }
+}
 
 // Local indices the monomial gate leaves in place with phase exactly 1.
 inline unsigned monomial_fixmask(const OpMonomial& op, unsigned m) {
@@ -520,7 +537,9 @@ inline void dm_orient(OpMix2& op, bool transposed) {
     if (transposed) for (auto& z : op.u) z = cconj(z);
 }
 inline void dm_orient(OpMonomial& op, bool transposed) {
-    if (transposed) for (auto& z : op.phase) z = cconj(z);
+    if (!transposed) return;
+    for (auto& z : op.phase) z = cconj(z);
+    for (auto& z : op.vph) z = cconj(z);
 }
 inline void dm_orient(OpSuper1& op, bool transposed) {
     if (!transposed) return;

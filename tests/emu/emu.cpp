@@ -264,6 +264,7 @@ int emu_dm_monomial(int layout, unsigned log_tile, double* rho, uint64_t len, un
     if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g, emu_max_v())) return -1;
     g.fixmask = monomial_fixmask(op, 1u << k);
     g.fixrows = dm_fixed_rows(g);
+    dm_monomial_tables(op, g);
     return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
 }
 
