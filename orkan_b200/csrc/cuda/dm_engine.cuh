@@ -476,27 +476,47 @@ struct OpSuper1 {
 // Monomial gate U|x> with an involutive permutation (X, Y, CX, CY, SWAP, CCX ...):
 // (U psi)[y] = phase[y] * psi[src[y]] on the local index, src[src[y]] == y.
 // Element pairs (y, z) <-> (src y, src z) are 2-cycles; the thread owning the
-// smaller flat index of a pair updates both.  The permutation and the phases are looked up
-// per virtual index (tables sig / vph of the block, filled once per launch by
-// dm_monomial_tables) instead of being assembled from the gate bits per element.
+// smaller flat index of a pair updates both.
+// The gates of the library are controlled flips: on virtual indices the image of x is
+// x ^ tmask when cond(x) holds -- all bits of cmask set (X, Y, CX, CY, CCX), or the two
+// bits of tmask different (SWAP) -- with phase p1 / p0 (target bit of x set / clear) where
+// it holds and 1 elsewhere.  dm_monomial_tables recognises that form (flip = 1) and the
+// operator then needs a few bit operations per element; other involutions use the local
+// index tables src / phase.
 struct OpMonomial {
     unsigned src[8];
     double2 phase[8];
-    unsigned char sig[kDmMaxV];   // virtual index -> virtual index of its image
-    double2 vph[kDmMaxV];         // phase of the local index of virtual index x
+    int flip;              // 1: controlled-flip form below
+    int parity;            // cond(x): 0 all cmask bits set, 1 the two tmask bits differ
+    unsigned cmask, tmask, tbit;
+    double2 p0, p1;
+    ORKAN_HD unsigned image(unsigned x, const DmGeom& g, double2* ph) const {
+        if (flip) {
+            const bool c = parity ? (((x & tmask) != 0) && ((x & tmask) != tmask)) : ((x & cmask) == cmask);
+            *ph = c ? ((x & tbit) ? p1 : p0) : c2(1.0, 0.0);
+            return c ? x ^ tmask : x;
+        }
+        const unsigned l = dm_get_local(x, g.vbit, g.k);
+        *ph = phase[l];
+        return dm_set_local(x, src[l], g.vbit, g.k);
+    }
     ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
         const unsigned V = g.V(), P = g.P(), lv = g.ls + g.h;
         const unsigned total = V * V;
         for (unsigned f = tid; f < total; f += nthr) {
             const unsigned r = f >> lv, c = f & (V - 1);
-            const unsigned r2 = sig[r], c2i = sig[c];
+            double2 pr, pc;
+            const unsigned r2 = image(r, g, &pr), c2i = image(c, g, &pc);
             const unsigned f2 = (r2 << lv) + c2i;
             if (f2 < f) continue;
-            const double2 fa = cmulc(vph[r], vph[c]);
+            const double2 fa = cmulc(pr, pc);
             if (f2 == f) {
                 vb[r * P + c] = cmul(fa, vb[r * P + c]);
             } else {
-                const double2 fb = cmulc(vph[r2], vph[c2i]);
+                double2 pr2, pc2;
+                image(r2, g, &pr2);
+                image(c2i, g, &pc2);
+                const double2 fb = cmulc(pr2, pc2);
                 const double2 va = vb[r * P + c], vb2 = vb[r2 * P + c2i];
                 vb[r * P + c] = cmul(fa, vb2);
                 vb[r2 * P + c2i] = cmul(fb, va);
@@ -505,16 +525,39 @@ struct OpMonomial {
     }
 };
 
-// Per-virtual-index tables of a monomial gate for the geometry g.
+// Recognise the controlled-flip form of op for the geometry g (see OpMonomial).
 inline void dm_monomial_tables(OpMonomial& op, const DmGeom& g) {
-    for (unsigned x = 0; x < kDmMaxV; ++x) {
-        if (x < g.V()) {
-            const unsigned l = dm_get_local(x, g.vbit, g.k);
-            op.sig[x] = (unsigned char)dm_set_local(x, op.src[l], g.vbit, g.k);
-            op.vph[x] = op.phase[l];
-        } else {
-            op.sig[x] = (unsigned char)x;
-            op.vph[x] = c2(1.0, 0.0);
+    const unsigned k = g.k, m = 1u << k;
+    op.flip = 0;
+    op.parity = 0;
+    op.cmask = op.tmask = op.tbit = 0;
+    op.p0 = op.p1 = c2(1.0, 0.0);
+    auto vmask = [&](unsigned j) { return 1u << g.vbit[j]; };
+    // target = last gate qubit (local bit 0), controls = the others
+    bool ctrl = true;
+    for (unsigned l = 0; l < m && ctrl; ++l) {
+        const bool on = (l | 1u) == m - 1;                       // every control bit set
+        const unsigned want = on ? (l ^ 1u) : l;
+        if (op.src[l] != want) ctrl = false;
+        if (!on && !(op.phase[l].x == 1.0 && op.phase[l].y == 0.0)) ctrl = false;
+    }
+    if (ctrl) {
+        op.flip = 1;
+        for (unsigned j = 0; j + 1 < k; ++j) op.cmask |= vmask(j);
+        op.tmask = op.tbit = vmask(k - 1);
+        op.p0 = op.phase[m - 2];
+        op.p1 = op.phase[m - 1];
+        return;
+    }
+    // SWAP of two qubits with unit phases
+    if (k == 2 && op.src[0] == 0 && op.src[1] == 2 && op.src[2] == 1 && op.src[3] == 3) {
+        bool unit = true;
+        for (unsigned l = 0; l < 4; ++l) unit = unit && op.phase[l].x == 1.0 && op.phase[l].y == 0.0;
+        if (unit) {
+            op.flip = 1;
+            op.parity = 1;
+            op.tmask = vmask(0) | vmask(1);
+            op.tbit = vmask(1);
         }
     }
 }
@@ -539,7 +582,8 @@ inline void dm_orient(OpMix2& op, bool transposed) {
 inline void dm_orient(OpMonomial& op, bool transposed) {
     if (!transposed) return;
     for (auto& z : op.phase) z = cconj(z);
-    for (auto& z : op.vph) z = cconj(z);
+    op.p0 = cconj(op.p0);
+    op.p1 = cconj(op.p1);
 }
 inline void dm_orient(OpSuper1& op, bool transposed) {
     if (!transposed) return;
