@@ -501,6 +501,8 @@ struct OpMonomial {
         return dm_set_local(x, src[l], g.vbit, g.k);
     }
     ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
+        if (flip && !parity) { flip_groups(g, vb, tid, nthr); return; }
+        if (flip) { swap_groups(g, vb, tid, nthr); return; }
         const unsigned V = g.V(), P = g.P(), lv = g.ls + g.h;
         const unsigned total = V * V;
         for (unsigned f = tid; f < total; f += nthr) {
@@ -521,6 +523,52 @@ struct OpMonomial {
                 vb[r * P + c] = cmul(fa, vb2);
                 vb[r2 * P + c2i] = cmul(fb, va);
             }
+        }
+    }
+    // Controlled flips: 2 x 2 groups over the target bit.  The control bits are the same for
+    // both rows (columns) of a group, so the rows are exchanged (with phases p0, p1) when the
+    // rows satisfy the condition, the columns likewise; groups where neither does are left
+    // untouched (not read, not written).
+    ORKAN_HD void flip_groups(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
+        const unsigned P = g.P(), lh = g.ls + g.h - 1, tpos = ctz64(tmask);
+        const unsigned groups = 1u << (2 * lh);
+        const double2 one = c2(1.0, 0.0);
+        for (unsigned t = tid; t < groups; t += nthr) {
+            const unsigned r0 = (unsigned)insert0(t >> lh, tpos), c0 = (unsigned)insert0(t & ((1u << lh) - 1), tpos);
+            const bool cr = (r0 & cmask) == cmask, cc = (c0 & cmask) == cmask;
+            if (!cr && !cc) continue;
+            const unsigned r1 = r0 | tmask, c1 = c0 | tmask;
+            const double2 x00 = vb[r0 * P + c0], x01 = vb[r0 * P + c1];
+            const double2 x10 = vb[r1 * P + c0], x11 = vb[r1 * P + c1];
+            // row phases (target bit 0 / 1 of the new row) and column phases
+            const double2 pr0 = cr ? p0 : one, pr1 = cr ? p1 : one, pc0 = cc ? p0 : one, pc1 = cc ? p1 : one;
+            const double2 s00 = cr ? (cc ? x11 : x10) : (cc ? x01 : x00);
+            const double2 s01 = cr ? (cc ? x10 : x11) : (cc ? x00 : x01);
+            const double2 s10 = cr ? (cc ? x01 : x00) : (cc ? x11 : x10);
+            const double2 s11 = cr ? (cc ? x00 : x01) : (cc ? x10 : x11);
+            vb[r0 * P + c0] = cmul(cmulc(pr0, pc0), s00);
+            vb[r0 * P + c1] = cmul(cmulc(pr0, pc1), s01);
+            vb[r1 * P + c0] = cmul(cmulc(pr1, pc0), s10);
+            vb[r1 * P + c1] = cmul(cmulc(pr1, pc1), s11);
+        }
+    }
+    // SWAP: 4 x 4 groups over the two bits (index order 00, a, b, ab); rows and columns a <-> b.
+    ORKAN_HD void swap_groups(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
+        const unsigned P = g.P(), lq = g.ls + g.h - 2;
+        const unsigned lo = tmask & (0u - tmask), hi = tmask ^ lo;
+        const unsigned asc[2] = {(unsigned)ctz64(lo), (unsigned)ctz64(hi)};
+        const unsigned groups = 1u << (2 * lq);
+        const unsigned sg[4] = {0, 2, 1, 3};                  // 00, lo, hi, both -> image
+        for (unsigned t = tid; t < groups; t += nthr) {
+            const unsigned rb = (unsigned)insert0_sorted(t >> lq, asc, 2);
+            const unsigned cb = (unsigned)insert0_sorted(t & ((1u << lq) - 1), asc, 2);
+            const unsigned off[4] = {0, lo, hi, lo | hi};
+            double2 x[4][4];
+            for (unsigned i = 0; i < 4; ++i)
+                for (unsigned j = 0; j < 4; ++j) x[i][j] = vb[(rb | off[i]) * P + (cb | off[j])];
+            for (unsigned i = 0; i < 4; ++i)
+                for (unsigned j = 0; j < 4; ++j)
+                    if (sg[i] != i || sg[j] != j) vb[(rb | off[i]) * P + (cb | off[j])] = x[sg[i]][sg[j]];
         }
     }
 };
