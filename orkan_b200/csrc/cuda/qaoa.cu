@@ -53,12 +53,13 @@ template <unsigned NT, class CostT, unsigned RING>
 __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_qaoa_pass(QaoaPass P, QaoaTables T) {
     extern __shared__ __align__(16) unsigned char smem_q[];
     const unsigned lc = P.kind == kQaoaFull ? P.plan.q1 : P.C;
+    const idx_t cmask = (idx_t(1) << P.li) - 1;
     auto fill = [&](idx_t w, unsigned slot) {
-        const QaoaInst I = P.inst[qaoa_find(P.inst, P.ninst, w)];
+        const QaoaInst I = P.inst[w >> P.li];
         const QaoaPlan& pl = P.plan;
         const QaoaSmem<CostT> S = qaoa_smem_at<CostT>(smem_q, lc, NT, RING, slot);
-        qaoa_fill<CostT>(P, I, pl, QaoaDevPsi{I.psi}, QaoaDevCost<CostT>{static_cast<const CostT*>(I.cost)},
-                         w - I.item0, S, threadIdx.x, NT);
+        qaoa_fill<CostT>(P, T, I, pl, QaoaDevPsi{I.psi}, QaoaDevCost<CostT>{static_cast<const CostT*>(I.cost)},
+                         w & cmask, S, threadIdx.x, NT);
     };
     unsigned slot = 0;
     idx_t w = blockIdx.x;
@@ -74,12 +75,12 @@ __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_qaoa_pass(QaoaPass P
             qaoa_cp_wait<0>();
         }
         __syncthreads();
-        const QaoaInst I = P.inst[qaoa_find(P.inst, P.ninst, w)];
+        const QaoaInst I = P.inst[w >> P.li];
         const QaoaPlan& pl = P.plan;
         const QaoaSmem<CostT> S = qaoa_smem_at<CostT>(smem_q, lc, NT, RING, slot);
         const unsigned nst = qaoa_stages(pl);
         for (unsigned st = 0; st < nst; ++st) {
-            qaoa_stage<CostT>(P, T, I, pl, QaoaDevPsi{I.psi}, w - I.item0, st, S, threadIdx.x, NT);
+            qaoa_stage<CostT>(P, T, I, pl, QaoaDevPsi{I.psi}, w & cmask, st, S, threadIdx.x, NT);
             __syncthreads();
         }
         if (RING == 2) {

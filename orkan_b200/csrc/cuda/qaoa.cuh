@@ -138,17 +138,6 @@ ORKAN_HD unsigned qaoa_high_slot(unsigned r, unsigned R, unsigned lw, unsigned B
     return row | (col << R);
 }
 
-// Work item w -> position in the pass's instance list (binary search over item0).
-ORKAN_HD unsigned qaoa_find(const QaoaInst* inst, unsigned ninst, idx_t w) {
-    unsigned lo = 0, hi = ninst;
-    while (hi - lo > 1) {
-        const unsigned mid = (lo + hi) >> 1;
-        if (inst[mid].item0 <= w) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
 // Shared-memory position of slot s: one padding slot after every 16.  With the mixed qubits
 // in groups of 4 slot bits starting at bit 0, 4, 8 or 12, the slots of a register set are
 // then equally spaced (base + j 2^b0 sits at pad(base) + j (2^b0 + 2^(b0-4)), or + j for
@@ -256,12 +245,20 @@ struct QaoaPass {
     unsigned C;            // log2 of the chunk (amplitudes per item)
     unsigned kind;         // QaoaKind
     QaoaPlan plan;         // qaoa_plan(n, C, kind, p, pass) of the launch's qubit count
+    unsigned li;           // log2 of the work items per instance: item w is chunk w mod 2^li
+                           // of instance w >> li of the list (every instance has n qubits)
+    int table_layer;       // the layer of the pass's one phase (low and high passes), whose
+                           // table byte-cost launches stage in shared memory; -1: none
     QaoaStage stage[kQaoaStageTable];   // qaoa_reg_stage(plan, r) for r < nreg <= kQaoaStageTable
 };
 
 // Fill in the plan and the stage table of a pass of n-qubit instances.
 ORKAN_HD void qaoa_pass_setup(QaoaPass& P, unsigned n) {
     P.plan = qaoa_plan(n, P.C, P.kind, P.p, P.pass);
+    P.li = P.kind == kQaoaFull ? 0u : n - P.C;
+    P.table_layer = P.kind == kQaoaFull ? -1
+                    : P.plan.phase_load >= 0 ? (int)P.plan.layer0 + P.plan.phase_load
+                    : P.plan.segs > 1 ? (int)P.plan.layer0 + 1 : -1;
     for (unsigned r = 0; r < kQaoaStageTable; ++r)
         P.stage[r] = r < P.plan.nreg ? qaoa_reg_stage(P.plan, r) : QaoaStage{};
 }
@@ -299,14 +296,20 @@ template <class CostT>
 struct QaoaSmem {
     double2* vb;
     typename QaoaCostWord<CostT>::type* cw;
+    double2* tab;          // byte costs: the staged phase table of the pass's phase layer
     double* red;
 };
+
+// Phase-table entries a buffer holds: kQaoaMaxTable for byte costs, none for FP64 costs.
+template <class CostT>
+ORKAN_HD constexpr unsigned qaoa_table_slots() { return std::is_same<CostT, double>::value ? 0u : kQaoaMaxTable; }
 
 // Bytes of one buffer, rounded up to 128 so that every buffer, its cost words and the
 // reduction array after the last buffer keep the alignment of the shared-memory base.
 template <class CostT>
 ORKAN_HD size_t qaoa_buffer_bytes(unsigned C) {
-    const size_t b = (size_t(16) + sizeof(typename QaoaCostWord<CostT>::type)) * qaoa_padded(C);
+    const size_t b = (size_t(16) + sizeof(typename QaoaCostWord<CostT>::type)) * qaoa_padded(C) +
+                     size_t(16) * qaoa_table_slots<CostT>();
     return (b + 127) & ~size_t(127);
 }
 
@@ -317,8 +320,9 @@ template <class CostT>
 ORKAN_HD bool qaoa_smem_aligned(unsigned C, unsigned ring) {
     const size_t w = sizeof(typename QaoaCostWord<CostT>::type);
     for (unsigned slot = 0; slot < ring; ++slot) {
-        const size_t vb = qaoa_buffer_bytes<CostT>(C) * slot, cw = vb + size_t(16) * qaoa_padded(C);
-        if (vb % 16 || cw % w) return false;
+        const size_t vb = qaoa_buffer_bytes<CostT>(C) * slot, tab = vb + size_t(16) * qaoa_padded(C);
+        const size_t cw = tab + size_t(16) * qaoa_table_slots<CostT>();
+        if (vb % 16 || tab % 16 || cw % w) return false;
     }
     return (qaoa_buffer_bytes<CostT>(C) * ring) % 8 == 0;
 }
@@ -331,7 +335,10 @@ ORKAN_HD QaoaSmem<CostT> qaoa_smem_at(unsigned char* base, unsigned C, unsigned 
     QaoaSmem<CostT> S;
     unsigned char* b = base + qaoa_buffer_bytes<CostT>(C) * slot;
     S.vb = reinterpret_cast<double2*>(b);
-    S.cw = reinterpret_cast<typename QaoaCostWord<CostT>::type*>(b + size_t(16) * qaoa_padded(C));
+    // [amplitudes, 16 B each][phase table, 16 B each][cost words]: every region aligned
+    S.tab = qaoa_table_slots<CostT>() ? reinterpret_cast<double2*>(b + size_t(16) * qaoa_padded(C)) : nullptr;
+    S.cw = reinterpret_cast<typename QaoaCostWord<CostT>::type*>(
+        b + size_t(16) * (qaoa_padded(C) + qaoa_table_slots<CostT>()));
     S.red = reinterpret_cast<double*>(base + qaoa_buffer_bytes<CostT>(C) * ring);
     (void)nthr;
     return S;
@@ -342,9 +349,13 @@ ORKAN_HD QaoaSmem<CostT> qaoa_smem_at(unsigned char* base, unsigned C, unsigned 
 // threads copy consecutive amplitudes.  Mem::cp16(dst, x) copies amplitude x,
 // CostMem::cpw(dst, x) the cost word of amplitude x.
 template <class CostT, class Mem, class CostMem>
-ORKAN_HD void qaoa_fill(const QaoaPass& P, const QaoaInst& I, const QaoaPlan& pl, const Mem& psi, const CostMem& cost,
-                        idx_t chunk, const QaoaSmem<CostT>& S, unsigned tid, unsigned nthr) {
+ORKAN_HD void qaoa_fill(const QaoaPass& P, const QaoaTables& T, const QaoaInst& I, const QaoaPlan& pl, const Mem& psi,
+                        const CostMem& cost, idx_t chunk, const QaoaSmem<CostT>& S, unsigned tid, unsigned nthr) {
     const unsigned cnt = 1u << qaoa_lc(I.n, P.C, P.kind);
+    if (qaoa_table_slots<CostT>() && P.table_layer >= 0) {    // the phase table of the pass
+        const double2* row = T.phase + ((idx_t)I.pos * P.p + (unsigned)P.table_layer) * T.tstride;
+        for (unsigned e = tid; e < T.tstride; e += nthr) psi.cpg(S.tab + e, row + e);
+    }
     if (P.kind != kQaoaHigh) {                     // contiguous chunk: equally spaced copies
         const idx_t x0 = P.kind == kQaoaLow ? chunk << P.C : 0;
         for (unsigned e = tid; e < cnt; e += nthr) {
@@ -406,7 +417,7 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
         if (sg.pre_phase >= 0) {
             const unsigned layer = pl.layer0 + (unsigned)sg.pre_phase;
             const double gam = P.gamma[row + layer];
-            const double2* tb = T.phase + (row + layer) * T.tstride;
+            const double2* tb = (int)layer == P.table_layer && S.tab ? S.tab : T.phase + (row + layer) * T.tstride;
 #pragma unroll
             for (unsigned j = 0; j < NV; ++j) v[j] = qaoa_apply_phase(qaoa_phase<CostT>(cost_of(j), gam, tb), v[j]);
         }
@@ -443,7 +454,8 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
             if (t < sg.t1) {                                  // scale of segment t, phase of the next layer
                 const double f = rx.f[P.kind];
                 const double gam = P.gamma[row + layer + 1];
-                const double2* tb = T.phase + (row + layer + 1) * T.tstride;
+                const double2* tb = (int)layer + 1 == P.table_layer && S.tab ? S.tab
+                                                                             : T.phase + (row + layer + 1) * T.tstride;
 #pragma unroll
                 for (unsigned j = 0; j < NV; ++j) {
                     const double2 ph = qaoa_phase<CostT>(cost_of(j), gam, tb);
@@ -517,6 +529,10 @@ struct QaoaDevPsi {
     __device__ __forceinline__ void cp16(double2* dst, idx_t i) const {
         const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(p + i) : "memory");
+    }
+    __device__ __forceinline__ void cpg(double2* dst, const double2* src) const {   // a table entry
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
     }
 };
 template <class CostT>

@@ -53,6 +53,8 @@ struct EmuMem {
         ++reads[i];
         *dst = p[i];
     }
+    // asynchronous copy of a phase-table entry (not state storage): lands immediately here
+    void cpg(double2* dst, const double2* src) const { *dst = *src; }
     // bulk copies of the GPU path (TMA): n consecutive elements, land immediately here
     void bulk_load(double2* sdst, idx_t i, unsigned n, void*) const {
         for (unsigned k = 0; k < n; ++k) sdst[k] = ld(i + k);
@@ -219,7 +221,7 @@ int run_qaoa(unsigned n, const CostT* cost, unsigned p, const double* gamma, con
         std::vector<unsigned char> smem(qaoa_smem_bytes<CostT>(P.C, nthr, 1));
         const QaoaSmem<CostT> S = qaoa_smem_at<CostT>(smem.data(), P.C, nthr, 1, 0);
         for (idx_t w = 0; w < P.items; ++w) {
-            for (unsigned t = 0; t < nthr; ++t) qaoa_fill<CostT>(P, I, pl, mem, cmem, w, S, t, nthr);
+            for (unsigned t = 0; t < nthr; ++t) qaoa_fill<CostT>(P, T, I, pl, mem, cmem, w, S, t, nthr);
             for (unsigned st = 0; st < qaoa_stages(pl); ++st)
                 for (unsigned t = 0; t < nthr; ++t) qaoa_stage<CostT>(P, T, I, pl, mem, w, st, S, t, nthr);
         }
