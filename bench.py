@@ -51,6 +51,8 @@ def parse_args():
     ap.add_argument("--batch-instances", type=int, default=4096, help="instances of the batched QAOA leg (0: skip)")
     ap.add_argument("--surrogate-pairs", type=int, default=8192,
                     help="training pairs of the surrogate leg (65536: the full configuration; 0: skip)")
+    ap.add_argument("--channel-qubits", type=int, default=13,
+                    help="density-matrix qubits of the Kraus-channel leg (0: skip)")
     ap.add_argument("--noisy-pairs", type=int, default=0,
                     help="training pairs of the noisy (density-matrix) surrogate leg (0: skip)")
     return ap.parse_args()
@@ -276,6 +278,59 @@ def run_reference(args):
     return 0
 
 
+
+
+# ---------------------------------------------------------------------------------------
+# Kraus-channel leg: 13 q tiled and packed density matrices, four channel kinds per qubit
+# ---------------------------------------------------------------------------------------
+def channels_leg(args, ork, clocks_cls, local):
+    import torch
+    from orkan_b200 import traffic as T
+    from orkan_b200 import workloads as W
+    n = args.channel_qubits
+    chans = W.channel_set(n, seed=3)
+    sops = [(label, ork.superop(kr), q) for label, kr, q in chans]
+    out = {"metric": "channel GB/s", "unit": "GB/s", "dtype": "f64",
+           "config": {"workload": f"{n} q tiled and packed density matrices (Dirichlet(1,1,1,1) mixtures of 4 "
+                                  f"Gaussian states): depolarizing p~U[0,0.1], amplitude damping g~U[0,0.2], phase "
+                                  f"damping l~U[0,0.2] and a random 4-Kraus CPTP channel on every qubit, as "
+                                  f"superoperators; then mean and matel_diag (PURE companion state) of a U[-1,1] "
+                                  f"observable", "channels_per_step": len(sops)}}
+    peak, peak_kind = measured_peak()
+    obs = W.uniform_obs_torch(n, seed=9)
+    ones = torch.ones(1 << n, dtype=torch.float64, device="cuda")
+    for kind in ("tiled", "packed"):
+        st = ork.state(kind, n)
+        W.fill_state_on_device(ork, st, kind, n, seed=5, log_tile=5)
+        nbytes = sum(T.gate_bytes(kind, n, "h", (q,), 5) for _, _, q in sops)    # dense: every element changes
+        for label, sop, q in sops[:8]:                                             # warm-up
+            ork.channel_1q(st, sop, q)
+        torch.cuda.synchronize()
+        clk = clocks_cls(local)
+        clk.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(max(1, args.steps)):
+            for label, sop, q in sops:
+                ork.channel_1q(st, sop, q)
+        e1.record()
+        torch.cuda.synchronize()
+        clocks = clk.stop()
+        ms = e0.elapsed_time(e1) / max(1, args.steps)
+        m = ork.mean(st, obs.data_ptr())
+        out[kind] = {"value": nbytes / (ms * 1e-3) / 1e9, "ms_per_step": ms, "algorithmic_bytes_per_step": nbytes,
+                     "frac_of_peak": nbytes / (ms * 1e-3) / 1e9 / peak, "peak_source": peak_kind,
+                     "trace_after": ork.mean(st, ones.data_ptr()), "mean": m, "clocks": clocks}
+        ork.free(st)
+    # observables: mean on both layouts above; matel_diag is PURE-only in the reference
+    pst, ket = ork.state("pure", n), ork.state("pure", n)
+    W.fill_state_on_device(ork, pst, "pure", n, seed=6, log_tile=5)
+    W.fill_state_on_device(ork, ket, "pure", n, seed=7, log_tile=5)
+    out["matel_diag_pure"] = [float(x) for x in (lambda z: (z.real, z.imag))(ork.matel_diag(pst, ket, obs.data_ptr()))]
+    ork.free(pst)
+    ork.free(ket)
+    out["value"] = 0.5 * (out["tiled"]["value"] + out["packed"]["value"])
+    return out
 
 # ---------------------------------------------------------------------------------------
 # batched QAOA leg: 4096 MaxCut instances of 16..24 qubits, p = 4 (include/orkan_batch.h)
@@ -642,7 +697,9 @@ def run_gpu(args):
 
     for st in states.values():
         ork.free(st)
-    batched = surrogate = noisy = None
+    batched = surrogate = noisy = channels = None
+    if rank == 0 and world == 1 and args.channel_qubits > 0:
+        channels = channels_leg(args, ork, ClockSampler, local)
     if rank == 0 and world == 1 and args.batch_instances > 0:
         batched = batched_leg(args, ork, ClockSampler, local)
     if rank == 0 and world == 1 and args.surrogate_pairs > 0:
@@ -663,7 +720,7 @@ def run_gpu(args):
                            "parallelism": f"replicas x{world}"},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": launches, "kernel_classes": classes, "by_gate": gates,
-                "batched": batched, "surrogate": surrogate, "surrogate_noisy": noisy}
+                "channels": channels, "batched": batched, "surrogate": surrogate, "surrogate_noisy": noisy}
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

@@ -87,6 +87,31 @@ def sweep(n: int):
     return out
 
 
+def channel_set(n: int, seed: int):
+    """The Kraus-channel throughput configuration on n qubits: on every qubit a depolarizing
+    channel (p ~ U[0, 0.1], p/4 form), amplitude damping (gamma ~ U[0, 0.2]), phase damping
+    (lambda ~ U[0, 0.2]) and a random 4-operator CPTP channel (the 2 x 2 blocks of the QR
+    isometry of a Gaussian complex 8 x 2 matrix).  Returns [(label, kraus, qubit)]."""
+    rng = np.random.default_rng(4321 + n)
+    out = []
+    x = np.array([[0, 1], [1, 0]], dtype=np.complex128)
+    y = np.array([[0, -1j], [1j, 0]], dtype=np.complex128)
+    z = np.array([[1, 0], [0, -1]], dtype=np.complex128)
+    for q in range(n):
+        p = rng.uniform(0.0, 0.1)
+        a, b = math.sqrt(1.0 - 3.0 * p / 4.0), math.sqrt(p / 4.0)
+        out.append(("depolarizing", [a * np.eye(2), b * x, b * y, b * z], q))
+        g = rng.uniform(0.0, 0.2)
+        out.append(("amplitude_damping", [np.array([[1, 0], [0, math.sqrt(1 - g)]], dtype=np.complex128),
+                                          np.array([[0, math.sqrt(g)], [0, 0]], dtype=np.complex128)], q))
+        lam = rng.uniform(0.0, 0.2)
+        out.append(("phase_damping", [np.array([[1, 0], [0, math.sqrt(1 - lam)]], dtype=np.complex128),
+                                      np.array([[0, 0], [0, math.sqrt(lam)]], dtype=np.complex128)], q))
+        iso, _ = np.linalg.qr(rng.standard_normal((8, 2)) + 1j * rng.standard_normal((8, 2)))
+        out.append(("random_cptp", [iso[2 * i:2 * i + 2, :] for i in range(4)], q))
+    return out
+
+
 # ---------------------------------------------------------------------------------------
 # device-side generation of the large benchmark states (torch is only the RNG/plumbing)
 # ---------------------------------------------------------------------------------------
