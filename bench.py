@@ -280,6 +280,45 @@ def run_reference(args):
 
 
 
+
+# ---------------------------------------------------------------------------------------
+# observables on the sweep's states: mean, matel_diag (PURE), exp_diag
+# ---------------------------------------------------------------------------------------
+def observables_leg(args, ork, states, obs_dev):
+    import torch
+    from orkan_b200 import traffic as T
+    peak, peak_kind = measured_peak()
+    out = {"unit": "GB/s", "peak": peak, "peak_source": peak_kind}
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    for kind, st in states.items():
+        n = args.pure_qubits if kind == "pure" else args.mixed_qubits
+        o = obs_dev[kind].data_ptr()
+        res = {}
+        ms = timed(lambda: ork.mean(st, o))
+        res["mean"] = {"ms": ms, "GB/s": T.mean_bytes(kind, n) / (ms * 1e-3) / 1e9}
+        if kind == "pure":
+            ms = timed(lambda: ork.matel_diag(st, st, o))
+            b = 40 * (1 << n)                                   # bra, ket (16 B each) and obs (8 B)
+            res["matel_diag"] = {"ms": ms, "GB/s": b / (ms * 1e-3) / 1e9}
+        ms = timed(lambda: ork.exp_diag(st, o, 0.37), reps=3)
+        res["exp_diag"] = {"ms": ms, "GB/s": T.exp_diag_bytes(kind, n, 5) / (ms * 1e-3) / 1e9}
+        for v in res.values():
+            v["frac"] = v["GB/s"] / peak
+        out[kind] = res
+    return out
+
 # ---------------------------------------------------------------------------------------
 # Kraus-channel leg: 13 q tiled and packed density matrices, four channel kinds per qubit
 # ---------------------------------------------------------------------------------------
@@ -695,6 +734,7 @@ def run_gpu(args):
         # free device memory first is not needed; the CPU baseline runs on host memory
         cpu = cpu_baseline(plan, args.pure_qubits, args.mixed_qubits, args.cpu_seconds)
 
+    observables = observables_leg(args, ork, states, obs_dev) if rank == 0 else None
     for st in states.values():
         ork.free(st)
     batched = surrogate = noisy = channels = None
@@ -720,7 +760,7 @@ def run_gpu(args):
                            "parallelism": f"replicas x{world}"},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": launches, "kernel_classes": classes, "by_gate": gates,
-                "channels": channels, "batched": batched, "surrogate": surrogate, "surrogate_noisy": noisy}
+                "observables": observables, "channels": channels, "batched": batched, "surrogate": surrogate, "surrogate_noisy": noisy}
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
