@@ -51,6 +51,20 @@ struct GateFactor1 {
     }
 };
 
+// Controlled phase (CZ and every diagonal gate whose phases are 1 except on the all-ones
+// local index): phi(x) = ph when every bit of mask is set in x, else 1.  The element changes
+// when exactly one of r, c has them all: f = ph for r, conj(ph) for c.
+struct GateFactorCtrl {
+    unsigned long long mask;
+    double2 ph;
+    ORKAN_HD bool factor(idx_t r, idx_t c, double2* f) const {
+        const bool br = ((unsigned long long)r & mask) == mask, bc = ((unsigned long long)c & mask) == mask;
+        if (br == bc) return false;
+        *f = br ? ph : cconj(ph);
+        return true;
+    }
+};
+
 // k-qubit diagonal gate (k <= 3): phi(x) = phase[local(x)], local(x) = sum_j bit(x, q[j]) << (k-1-j);
 // f = phi(r) conj(phi(c)); equal local indices give |phi|^2 = 1 and are skipped.
 struct GateFactor {

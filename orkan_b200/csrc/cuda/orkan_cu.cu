@@ -250,6 +250,17 @@ int orkan_cu_dm_phase(int layout, unsigned log_tile, void* rho, unsigned n, unsi
         f1.ph1 = ld_c(phase, 1);
         return launch_phase(layout, log_tile, rho, n, f1, as_stream(stream));
     }
+    {                                                   // controlled phase (CZ): a mask test per element
+        bool ctrl = true;
+        for (unsigned y = 0; y + 1 < (1u << k); ++y) ctrl = ctrl && phase[2 * y] == 1.0 && phase[2 * y + 1] == 0.0;
+        if (ctrl) {
+            GateFactorCtrl fc;
+            fc.mask = 0;
+            for (unsigned j = 0; j < k; ++j) fc.mask |= 1ull << qubits[j];
+            fc.ph = ld_c(phase, (1u << k) - 1);
+            return launch_phase(layout, log_tile, rho, n, fc, as_stream(stream));
+        }
+    }
     GateFactor fac;
     fac.k = k;
     for (unsigned j = 0; j < 3; ++j) fac.q[j] = j < k ? qubits[j] : 0;

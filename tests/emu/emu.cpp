@@ -290,6 +290,18 @@ int emu_dm_phase(int layout, unsigned log_tile, double* rho, uint64_t len, unsig
         run_phase(layout, log_tile, mem, n, f1);
         return 0;
     }
+    {                                                   // controlled phase, as the GPU launcher picks it
+        bool ctrl = true;
+        for (unsigned y = 0; y + 1 < (1u << k); ++y) ctrl = ctrl && phase[2 * y] == 1.0 && phase[2 * y + 1] == 0.0;
+        if (ctrl) {
+            GateFactorCtrl fc;
+            fc.mask = 0;
+            for (unsigned j = 0; j < k; ++j) fc.mask |= 1ull << qubits[j];
+            fc.ph = ldc(phase, (1u << k) - 1);
+            run_phase(layout, log_tile, mem, n, fc);
+            return 0;
+        }
+    }
     GateFactor fac;
     fac.k = k;
     for (unsigned j = 0; j < 3; ++j) fac.q[j] = j < k ? qubits[j] : 0;
