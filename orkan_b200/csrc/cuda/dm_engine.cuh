@@ -51,6 +51,8 @@ struct DmGeom {
                         // (monomial gates only; an element whose row and column are both
                         // fixed is unchanged and is neither loaded nor stored)
     unsigned long long fixrows;  // the same as a mask over virtual indices (dm_fixed_rows)
+    unsigned long long hcmask;   // controlled flips: control qubits above the sub-tile that are
+                                 // not pairing bits (one value per item's rows or columns)
     ORKAN_HD unsigned S() const { return 1u << ls; }
     ORKAN_HD unsigned V() const { return 1u << (ls + h); }
     ORKAN_HD unsigned P() const { return V() + 1; }    // smem row pitch (padded)
@@ -104,6 +106,7 @@ inline bool dm_geometry(unsigned n, unsigned k, const unsigned* qubits, unsigned
             g->items = g->nbase * (g->nbase + 1) / 2;
             g->fixmask = 0;
             g->fixrows = 0;
+            g->hcmask = 0;
             return true;
         }
         if (ls == 0) return false;
@@ -149,9 +152,17 @@ struct DmPos {
     int allvar;      // every fvar + p (p < S) is a fixed row/column of the gate
     unsigned bytes;  // bytes this position's lines bring in (for the transaction count)
     int pad_;
+    unsigned long long fmc;   // virtual indices fixed by the gate along the line-constant axis
+    unsigned long long pad2_;
 };
 constexpr unsigned kDmMaxPos = 64;                     // 4^h with h <= 3
-constexpr unsigned kDmPosBytes = kDmMaxPos * sizeof(DmPos);
+// One more descriptor slot after the positions holds the item's flags (cls field): bit 0
+// the staged block's major, bit 1 its minor indices meet the high controls of a controlled
+// flip (major = rows for the tiled layout, columns for the packed one); bit 2 the item is
+// left unchanged (neither its rows nor its columns meet them) and is skipped.
+constexpr unsigned kDmItemSlot = kDmMaxPos;
+constexpr unsigned kDmPosBytes = (kDmMaxPos + 1) * sizeof(DmPos);
+static_assert(sizeof(DmPos) == 80, "descriptor size");
 static_assert(kDmPosBytes % 16 == 0, "descriptor block keeps the staged block 16-byte aligned");
 
 // Virtual-index bit masks of fixed rows/columns (monomial gates): bit x set when local(x)
@@ -178,8 +189,8 @@ ORKAN_HD void dm_line_range(const DmPos& q, unsigned line, unsigned S, unsigned*
 }
 
 // A line every element of which the gate leaves in place: neither loaded nor stored.
-ORKAN_HD bool dm_line_skipped(unsigned long long fm, const DmPos& q, unsigned line) {
-    return fm && q.allvar && ((fm >> (q.fconst + line)) & 1ull);
+ORKAN_HD bool dm_line_skipped(const DmPos& q, unsigned line) {
+    return q.allvar && ((q.fmc >> (q.fconst + line)) & 1ull);
 }
 
 // Build the descriptors of item w (threads tid < 4^h, one position each).
@@ -192,7 +203,20 @@ ORKAN_HD void dm_setup(const Map& map, const DmGeom& g, idx_t w, DmPos* pd, unsi
     tri_unrank_f(w, &u, &v);
     const bool diag_item = (u == v);
     const idx_t rb = insert0_sorted(u, g.hb, h), cb = insert0_sorted(v, g.hb, h);
-    const unsigned long long fm = g.fixrows;
+    // high controls of a controlled flip: one value for all rows (columns) of the item; rows
+    // that do not meet them are all fixed
+    const unsigned long long hc = g.hcmask;
+    const bool rowc = ((unsigned long long)(rb << ls) & hc) == hc, colc = ((unsigned long long)(cb << ls) & hc) == hc;
+    const unsigned V = g.V();
+    const unsigned long long allv = V >= 64 ? ~0ull : ((1ull << V) - 1ull);
+    const unsigned long long fm_row = rowc ? g.fixrows : allv, fm_col = colc ? g.fixrows : allv;
+    const bool any_fixed = (fm_row | fm_col) != 0;
+    if (tid == 0) {
+        DmPos f{};
+        const bool maj = Map::kRowContig ? colc : rowc, mnr = Map::kRowContig ? rowc : colc;
+        f.cls = (maj ? 1 : 0) | (mnr ? 2 : 0) | ((!rowc && !colc) ? 4 : 0);
+        pd[kDmItemSlot] = f;
+    }
     const unsigned long long smask = (S >= 64) ? ~0ull : ((1ull << S) - 1ull);
     for (unsigned t = tid; t < npos; t += nthr) {
         const unsigned a = t >> h, b = t & ((1u << h) - 1);
@@ -206,6 +230,7 @@ ORKAN_HD void dm_setup(const Map& map, const DmGeom& g, idx_t w, DmPos* pd, unsi
         q.has_c = 0;
         q.mirror = 0;
         q.pad_ = 0;
+        q.pad2_ = 0;
         q.MB = Map::kRowContig ? bS : aS;
         q.mB = Map::kRowContig ? aS : bS;
         // virtual coordinates along a stored line: tiled line = virtual row (aS + line) for a
@@ -213,6 +238,9 @@ ORKAN_HD void dm_setup(const Map& map, const DmGeom& g, idx_t w, DmPos* pd, unsi
         const bool tr = (R < C);
         if (Map::kRowContig) { q.fconst = tr ? aS : bS; q.fvar = tr ? bS : aS; }
         else                 { q.fconst = tr ? bS : aS; q.fvar = tr ? aS : bS; }
+        const bool const_is_row = Map::kRowContig ? tr : !tr;
+        q.fmc = const_is_row ? fm_row : fm_col;
+        const unsigned long long fm_var = const_is_row ? fm_col : fm_row;
         if (R > C) {
             q.cls = kSubDirect;
             q.gbase = map.at(R, C);
@@ -234,7 +262,7 @@ ORKAN_HD void dm_setup(const Map& map, const DmGeom& g, idx_t w, DmPos* pd, unsi
         // tiled diagonal sub-tiles are stored as whole rows whose upper half is rebuilt from
         // the lower half, so none of their rows may be skipped
         const bool no_skip = Map::kMirrors && q.cls == kSubDiag;
-        q.allvar = (fm && !no_skip && ((fm >> q.fvar) & smask) == smask) ? 1 : 0;
+        q.allvar = (any_fixed && !no_skip && ((fm_var >> q.fvar) & smask) == smask) ? 1 : 0;
         // bytes the position's lines bring in: whole S x S sub-tile, or the lower half of a
         // diagonal one, less the lines skipped because every element in them is fixed
         unsigned bytes = 0;
@@ -242,7 +270,7 @@ ORKAN_HD void dm_setup(const Map& map, const DmGeom& g, idx_t w, DmPos* pd, unsi
             const unsigned full = q.cls == kSubDiag ? S * (S + 1) / 2 : S * S;
             bytes = full * 16u;
             if (q.allvar) {
-                const unsigned long long skip = (fm >> q.fconst) & smask;
+                const unsigned long long skip = (q.fmc >> q.fconst) & smask;
                 if (q.cls != kSubDiag) {
                     bytes -= (unsigned)popc64(skip) * S * 16u;
                 } else {                                   // packed diagonal: line j holds S - j
@@ -273,7 +301,7 @@ ORKAN_HD void dm_bulk_loads(const Mem& mem, const Map& map, const DmGeom& g, con
     for (unsigned t = tid; t < nlines; t += nthr) {
         const DmPos& q = pd[t >> ls];
         const unsigned line = t & (S - 1);
-        if (q.cls == kSubSkip || dm_line_skipped(g.fixrows, q, line)) continue;
+        if (q.cls == kSubSkip || dm_line_skipped(q, line)) continue;
         unsigned p0, p1;
         dm_line_range<Map>(q, line, S, &p0, &p1);
         mem.bulk_load(vb + (q.MB + (int)line) * (int)P + q.mB + (int)p0, dm_addr(map, q, line, p0), p1 - p0, bar);
@@ -288,7 +316,7 @@ ORKAN_HD void dm_bulk_stores(const Mem& mem, const Map& map, const DmGeom& g, co
     for (unsigned t = tid; t < nlines; t += nthr) {
         const DmPos& q = pd[t >> ls];
         const unsigned line = t & (S - 1);
-        if (q.cls == kSubSkip || dm_line_skipped(g.fixrows, q, line)) continue;
+        if (q.cls == kSubSkip || dm_line_skipped(q, line)) continue;
         unsigned p0 = 0, p1 = S;                            // tiled diagonal tiles: whole rows
         if (Map::kRowContig) dm_line_range<Map>(q, line, S, &p0, &p1);
         mem.bulk_store(dm_addr(map, q, line, p0), vb + (q.MB + (int)line) * (int)P + q.mB + (int)p0, p1 - p0);
@@ -335,7 +363,7 @@ ORKAN_HD void dm_mirror_stores(const Mem& mem, const Map& map, const DmGeom& g, 
         const DmPos& q = pd[t];
         for (unsigned e = tid; e < (1u << (2 * ls)); e += nthr) {
             const unsigned line = e >> ls, p = e & (S - 1);
-            if (dm_line_skipped(g.fixrows, q, line)) continue;
+            if (dm_line_skipped(q, line)) continue;
             mem.st(q.mbase + ((idx_t)p << map.log_tdim()) + line,
                    cconj(vb[(q.MB + (int)line) * (int)P + q.mB + (int)p]));
         }
@@ -397,7 +425,7 @@ ORKAN_HD unsigned dm_get_local(unsigned x, const unsigned* vbit, unsigned k) {
 // Dense 1-qubit unitary U (row-major u[2*r + c]):  G' = U G U^dagger on 2x2 groups.
 struct OpMix1 {
     double2 u[4];
-    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
+    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr, unsigned = 3u) const {
         const unsigned P = g.P(), lh = g.ls + g.h - 1, vbq = g.vbit[0];
         const unsigned groups = 1u << (2 * lh);
         for (unsigned t = tid; t < groups; t += nthr) {
@@ -422,7 +450,7 @@ struct OpMix1 {
 // Dense 2-qubit unitary U (row-major u[4*r + c], local index = 2*bit(q0) + bit(q1)).
 struct OpMix2 {
     double2 u[16];
-    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
+    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr, unsigned = 3u) const {
         const unsigned P = g.P(), lq = g.ls + g.h - 2;
         unsigned asc[2] = {g.vbit[0] < g.vbit[1] ? g.vbit[0] : g.vbit[1],
                            g.vbit[0] < g.vbit[1] ? g.vbit[1] : g.vbit[0]};
@@ -455,7 +483,7 @@ struct OpMix2 {
 // 1-qubit superoperator (row-major s[4*m + j]) on vec = (x00, x01, x10, x11).
 struct OpSuper1 {
     double2 s[16];
-    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
+    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr, unsigned = 3u) const {
         const unsigned P = g.P(), lh = g.ls + g.h - 1, vbq = g.vbit[0];
         const unsigned groups = 1u << (2 * lh);
         for (unsigned t = tid; t < groups; t += nthr) {
@@ -500,8 +528,8 @@ struct OpMonomial {
         *ph = phase[l];
         return dm_set_local(x, src[l], g.vbit, g.k);
     }
-    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
-        if (flip && !parity) { flip_groups(g, vb, tid, nthr); return; }
+    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr, unsigned iflags = 3u) const {
+        if (flip && !parity) { flip_groups(g, vb, tid, nthr, iflags); return; }
         if (flip) { swap_groups(g, vb, tid, nthr); return; }
         const unsigned V = g.V(), P = g.P(), lv = g.ls + g.h;
         const unsigned total = V * V;
@@ -529,13 +557,14 @@ struct OpMonomial {
     // both rows (columns) of a group, so the rows are exchanged (with phases p0, p1) when the
     // rows satisfy the condition, the columns likewise; groups where neither does are left
     // untouched (not read, not written).
-    ORKAN_HD void flip_groups(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr) const {
+    ORKAN_HD void flip_groups(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr, unsigned iflags) const {
+        const bool rowc = iflags & 1u, colc = (iflags >> 1) & 1u;     // high controls (major, minor)
         const unsigned P = g.P(), lh = g.ls + g.h - 1, tpos = ctz64(tmask);
         const unsigned groups = 1u << (2 * lh);
         const double2 one = c2(1.0, 0.0);
         for (unsigned t = tid; t < groups; t += nthr) {
             const unsigned r0 = (unsigned)insert0(t >> lh, tpos), c0 = (unsigned)insert0(t & ((1u << lh) - 1), tpos);
-            const bool cr = (r0 & cmask) == cmask, cc = (c0 & cmask) == cmask;
+            const bool cr = rowc && (r0 & cmask) == cmask, cc = colc && (c0 & cmask) == cmask;
             if (!cr && !cc) continue;
             const unsigned r1 = r0 | tmask, c1 = c0 | tmask;
             const double2 x00 = vb[r0 * P + c0], x01 = vb[r0 * P + c1];
@@ -573,49 +602,81 @@ struct OpMonomial {
     }
 };
 
-// Recognise the controlled-flip form of op for the geometry g (see OpMonomial).
-inline void dm_monomial_tables(OpMonomial& op, const DmGeom& g) {
-    const unsigned k = g.k, m = 1u << k;
-    op.flip = 0;
-    op.parity = 0;
-    op.cmask = op.tmask = op.tbit = 0;
-    op.p0 = op.p1 = c2(1.0, 0.0);
-    auto vmask = [&](unsigned j) { return 1u << g.vbit[j]; };
-    // target = last gate qubit (local bit 0), controls = the others
-    bool ctrl = true;
-    for (unsigned l = 0; l < m && ctrl; ++l) {
-        const bool on = (l | 1u) == m - 1;                       // every control bit set
-        const unsigned want = on ? (l ^ 1u) : l;
-        if (op.src[l] != want) ctrl = false;
-        if (!on && !(op.phase[l].x == 1.0 && op.phase[l].y == 0.0)) ctrl = false;
-    }
-    if (ctrl) {
-        op.flip = 1;
-        for (unsigned j = 0; j + 1 < k; ++j) op.cmask |= vmask(j);
-        op.tmask = op.tbit = vmask(k - 1);
-        op.p0 = op.phase[m - 2];
-        op.p1 = op.phase[m - 1];
-        return;
-    }
-    // SWAP of two qubits with unit phases
-    if (k == 2 && op.src[0] == 0 && op.src[1] == 2 && op.src[2] == 1 && op.src[3] == 3) {
-        bool unit = true;
-        for (unsigned l = 0; l < 4; ++l) unit = unit && op.phase[l].x == 1.0 && op.phase[l].y == 0.0;
-        if (unit) {
-            op.flip = 1;
-            op.parity = 1;
-            op.tmask = vmask(0) | vmask(1);
-            op.tbit = vmask(1);
-        }
-    }
-}
-
 // Local indices the monomial gate leaves in place with phase exactly 1.
 inline unsigned monomial_fixmask(const OpMonomial& op, unsigned m) {
     unsigned mask = 0;
     for (unsigned l = 0; l < m; ++l)
         if (op.src[l] == l && op.phase[l].x == 1.0 && op.phase[l].y == 0.0) mask |= 1u << l;
     return mask;
+}
+
+// Controlled-flip form of a k-qubit monomial gate: the last gate qubit (local bit 0) is the
+// target, the others are controls; local index l goes to l ^ 1 when every control bit is set
+// and stays in place with phase 1 otherwise (X, Y, CX, CY, CCX).
+inline bool monomial_is_controlled_flip(const OpMonomial& op, unsigned k) {
+    const unsigned m = 1u << k;
+    for (unsigned l = 0; l < m; ++l) {
+        const bool on = (l | 1u) == m - 1;                       // every control bit set
+        if (op.src[l] != (on ? (l ^ 1u) : l)) return false;
+        if (!on && !(op.phase[l].x == 1.0 && op.phase[l].y == 0.0)) return false;
+    }
+    return true;
+}
+
+// Host set-up of a monomial gate launch (geometry, fixed rows, operator form).
+//
+// A controlled flip is laid out over its target alone, so its block is as small as a
+// 1-qubit gate's: a control inside the block (below the sub-tile or on a pairing bit)
+// becomes a virtual-index condition (cmask), a control above it a condition on the item's
+// rows and columns (hcmask), and items that meet it in neither are skipped.  A SWAP with
+// unit phases uses the parity form; other gates the generic table over all their qubits.
+inline bool dm_monomial_setup(unsigned n, unsigned k, const unsigned* qubits, OpMonomial& op, unsigned ls_max,
+                              unsigned max_v_low, DmGeom* g) {
+    const unsigned m = 1u << k;
+    op.flip = 0;
+    op.parity = 0;
+    op.cmask = op.tmask = op.tbit = 0;
+    op.p0 = op.p1 = c2(1.0, 0.0);
+    if (k < 1 || k > 3) return false;
+    for (unsigned j = 0; j < k; ++j) {
+        if (qubits[j] >= n) return false;
+        for (unsigned i = 0; i < j; ++i) if (qubits[i] == qubits[j]) return false;
+    }
+    if (monomial_is_controlled_flip(op, k)) {
+        if (!dm_geometry(n, 1, &qubits[k - 1], ls_max, g, max_v_low)) return false;
+        op.flip = 1;
+        op.tmask = op.tbit = 1u << g->vbit[0];
+        op.p0 = op.phase[m - 2];
+        op.p1 = op.phase[m - 1];
+        for (unsigned j = 0; j + 1 < k; ++j) {
+            const unsigned q = qubits[j];
+            if (q < g->ls) { op.cmask |= 1u << q; continue; }
+            unsigned r = 0;
+            while (r < g->h && g->hb[r] != q - g->ls) ++r;
+            if (r < g->h) op.cmask |= 1u << (g->ls + r);           // a pairing bit of the block
+            else g->hcmask |= 1ull << q;
+        }
+        unsigned long long fr = 0;
+        if (op.cmask)
+            for (unsigned x = 0; x < g->V(); ++x)
+                if ((x & op.cmask) != op.cmask) fr |= 1ull << x;
+        g->fixrows = fr;
+        return true;
+    }
+    if (!dm_geometry(n, k, qubits, ls_max, g, max_v_low)) return false;
+    g->fixmask = monomial_fixmask(op, m);
+    g->fixrows = dm_fixed_rows(*g);
+    if (k == 2 && op.src[0] == 0 && op.src[1] == 2 && op.src[2] == 1 && op.src[3] == 3) {
+        bool unit = true;
+        for (unsigned l = 0; l < 4; ++l) unit = unit && op.phase[l].x == 1.0 && op.phase[l].y == 0.0;
+        if (unit) {
+            op.flip = 1;
+            op.parity = 1;
+            op.tmask = (1u << g->vbit[0]) | (1u << g->vbit[1]);
+            op.tbit = 1u << g->vbit[1];
+        }
+    }
+    return true;
 }
 
 // The packed layout stages rho^T: (U rho U^dagger)^T = conj(U) rho^T conj(U)^dagger, so its
@@ -652,11 +713,12 @@ template <class Map, class Mem, class Op>
 ORKAN_HD void dm_engine_item_phase(int phase, const Mem& mem, const Map& map, const DmGeom& g, const Op& op,
                                    idx_t w, DmPos* pd, double2* vb, unsigned tid, unsigned nthr) {
     const unsigned npos = 1u << (2 * g.h);
+    if (phase > 0 && (pd[kDmItemSlot].cls & 4)) return;     // item left unchanged
     switch (phase) {
         case 0: dm_setup(map, g, w, pd, tid, nthr); break;
         case 1: dm_bulk_loads(mem, map, g, pd, vb, nullptr, tid, nthr); break;
         case 2: dm_fixups<Map>(g, pd, vb, 0, dm_pass_mask<Map>(pd, npos, 0), tid, nthr); break;
-        case 3: op(g, vb, tid, nthr); break;
+        case 3: op(g, vb, tid, nthr, (unsigned)pd[kDmItemSlot].cls & 3u); break;
         case 4: dm_fixups<Map>(g, pd, vb, 1, dm_pass_mask<Map>(pd, npos, 1), tid, nthr); break;
         case 5: dm_bulk_stores(mem, map, g, pd, vb, tid, nthr); break;
         default: dm_mirror_stores(mem, map, g, pd, vb, dm_pass_mask<Map>(pd, npos, 2), tid, nthr); break;
@@ -736,6 +798,11 @@ __global__ void __launch_bounds__(kDmBlock) k_dm_engine(DevMemBulk mem, Map map,
     for (idx_t w = blockIdx.x; w < g.items; w += gridDim.x) {
         dm_setup(map, g, w, pd, tid, nthr);
         __syncthreads();                                   // descriptors ready (and barrier initialised)
+        const unsigned iflags = (unsigned)pd[kDmItemSlot].cls;
+        if (iflags & 4u) {                                 // nothing in the item changes
+            __syncthreads();                               // everyone has read the flags
+            continue;
+        }
         if (tid < 32) {                                     // warp 0 arms the barrier and issues the loads
             if (tid == 0) {
                 unsigned bytes = 0;
@@ -756,7 +823,7 @@ __global__ void __launch_bounds__(kDmBlock) k_dm_engine(DevMemBulk mem, Map map,
             dm_fixups<Map>(g, pd, vb, 0, fix0, tid, nthr);
             __syncthreads();
         }
-        op(g, vb, tid, nthr);
+        op(g, vb, tid, nthr, iflags & 3u);
         __syncthreads();
         if (fix1) {
             dm_fixups<Map>(g, pd, vb, 1, fix1, tid, nthr);

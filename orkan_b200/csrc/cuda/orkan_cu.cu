@@ -231,10 +231,8 @@ int orkan_cu_dm_monomial(int layout, unsigned log_tile, void* rho, unsigned n, u
         op.phase[y] = ld_c(phase, y);
     }
     DmGeom g;
-    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g, dm_max_v_low())) return (int)cudaErrorInvalidValue;
-    g.fixmask = monomial_fixmask(op, m);
-    g.fixrows = dm_fixed_rows(g);
-    dm_monomial_tables(op, g);
+    if (!dm_monomial_setup(n, k, qubits, op, ls_max_for(layout, log_tile), dm_max_v_low(), &g))
+        return (int)cudaErrorInvalidValue;
     return launch_engine_map(layout, log_tile, rho, n, g, op, as_stream(stream));
 }
 

@@ -119,7 +119,7 @@ template <class Map, class Op>
 void run_engine(const EmuMem& mem, const Map& map, const DmGeom& g, const Op& op) {
     const unsigned grid = grid_for(1, g.items, kSms * 32u);
     std::vector<double2> vb((size_t)g.V() * g.P());
-    std::vector<DmPos> pd(kDmMaxPos);
+    std::vector<DmPos> pd(kDmMaxPos + 1);
     Op o = op;
     dm_orient(o, !Map::kMirrors);           // the packed layout stages rho^T
     for (unsigned b = 0; b < grid; ++b) {
@@ -263,10 +263,7 @@ int emu_dm_monomial(int layout, unsigned log_tile, double* rho, uint64_t len, un
     for (unsigned y = 0; y < 8; ++y) { op.src[y] = y; op.phase[y] = c2(1.0, 0.0); }
     for (unsigned y = 0; y < (1u << k); ++y) { op.src[y] = src[y]; op.phase[y] = ldc(phase, y); }
     DmGeom g;
-    if (!dm_geometry(n, k, qubits, ls_max_for(layout, log_tile), &g, emu_max_v())) return -1;
-    g.fixmask = monomial_fixmask(op, 1u << k);
-    g.fixrows = dm_fixed_rows(g);
-    dm_monomial_tables(op, g);
+    if (!dm_monomial_setup(n, k, qubits, op, ls_max_for(layout, log_tile), emu_max_v(), &g)) return -1;
     return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
 }
 

@@ -98,6 +98,24 @@ def test_dm_gates_emulated(kind, lt, n):
 
 
 @pytest.mark.parametrize("kind,lt", LAYOUTS)
+@pytest.mark.parametrize("max_v", [8, 16])
+def test_dm_monomials_small_blocks_emulated(kind, lt, max_v, monkeypatch):
+    """Smaller block caps put more of a controlled flip's controls above the staged block
+    (item-level conditions, unchanged items skipped) and more gate qubits on pairing bits."""
+    monkeypatch.setenv("ORKAN_DM_MAX_V", str(max_v))
+    n = 7
+    rho = rand_rho(n, 300 + max_v)
+    st = R.to_storage(kind, rho, lt)
+    for g, qs, theta in gate_cases(n, max_ccx=120, seed=max_v):
+        if g not in ("x", "y", "cx", "cy", "ccx", "swap"):
+            continue
+        res = kemu.dm_gate(kind, lt, st, n, g, qs, theta)
+        exp = R.to_storage(kind, R.apply_mixed(rho, g, qs, theta), lt)
+        assert np.abs(res.out - exp).max() <= TOL, (g, qs)
+        check_engine_counts(kind, n, lt, res, g, qs)
+
+
+@pytest.mark.parametrize("kind,lt", LAYOUTS)
 @pytest.mark.parametrize("n", [2, 5, 7])
 def test_dm_generic_unitaries_emulated(kind, lt, n):
     rng = np.random.default_rng(7 + n)
