@@ -463,19 +463,26 @@ struct OpMix2 {
                 ri[l] = dm_set_local(rb, l, g.vbit, 2);
                 ci[l] = dm_set_local(cb, l, g.vbit, 2);
             }
-            double2 y[4][4];
-            for (unsigned r = 0; r < 4; ++r)
-                for (unsigned c = 0; c < 4; ++c) {
+            // the group's 16 elements belong to this thread alone: Y = U X column by column in
+            // place, then Z = Y U^dagger row by row (few values live at a time)
+            for (unsigned c = 0; c < 4; ++c) {
+                double2 x[4];
+                for (unsigned m = 0; m < 4; ++m) x[m] = vb[ri[m] * P + ci[c]];
+                for (unsigned r = 0; r < 4; ++r) {
                     double2 acc = c2(0.0, 0.0);
-                    for (unsigned m = 0; m < 4; ++m) acc = cadd(acc, cmul(u[4 * r + m], vb[ri[m] * P + ci[c]]));
-                    y[r][c] = acc;
-                }
-            for (unsigned r = 0; r < 4; ++r)
-                for (unsigned c = 0; c < 4; ++c) {
-                    double2 acc = c2(0.0, 0.0);
-                    for (unsigned m = 0; m < 4; ++m) acc = cadd(acc, cmulc(y[r][m], u[4 * c + m]));
+                    for (unsigned m = 0; m < 4; ++m) acc = cadd(acc, cmul(u[4 * r + m], x[m]));
                     vb[ri[r] * P + ci[c]] = acc;
                 }
+            }
+            for (unsigned r = 0; r < 4; ++r) {
+                double2 y[4];
+                for (unsigned m = 0; m < 4; ++m) y[m] = vb[ri[r] * P + ci[m]];
+                for (unsigned c = 0; c < 4; ++c) {
+                    double2 acc = c2(0.0, 0.0);
+                    for (unsigned m = 0; m < 4; ++m) acc = cadd(acc, cmulc(y[m], u[4 * c + m]));
+                    vb[ri[r] * P + ci[c]] = acc;
+                }
+            }
         }
     }
 };
@@ -708,7 +715,7 @@ ORKAN_HD size_t dm_stage_bytes(const DmGeom& g) { return kDmPosBytes + (size_t)g
 ORKAN_HD size_t dm_block_smem_bytes(const DmGeom& g) { return 16 + dm_stage_bytes(g); }
 
 // One work item, phase by phase (the CPU emulator runs each phase for all threads before
-// the next; the kernel below overlaps items with a two-stage pipeline).
+// the next; k_dm_engine runs the same phases with block barriers between them).
 template <class Map, class Mem, class Op>
 ORKAN_HD void dm_engine_item_phase(int phase, const Mem& mem, const Map& map, const DmGeom& g, const Op& op,
                                    idx_t w, DmPos* pd, double2* vb, unsigned tid, unsigned nthr) {
@@ -727,7 +734,7 @@ ORKAN_HD void dm_engine_item_phase(int phase, const Mem& mem, const Map& map, co
 constexpr int kDmPhases = 7;
 
 constexpr unsigned kDmBlock = 256;          // threads of an engine block
-constexpr unsigned kDmIssueThreads = 32;    // threads (one warp) that issue the bulk copies
+constexpr unsigned kDmIssueThreads = kDmBlock;   // threads that issue the bulk copies
 
 #ifdef __CUDACC__
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -777,11 +784,15 @@ __device__ __forceinline__ bool dm_wait_stage(unsigned long long* bar, unsigned 
     return false;
 }
 
+// Blocks per SM the register budget is held to: three blocks with a 64 x 64 staged block
+// fill the shared memory, and the bulk copies of one overlap the compute of the others.
+constexpr int kDmMinBlocks = 3;
+
 // Persistent engine: block b handles items b, b + G, b + 2G, ...  One item at a time per
 // block; with up to three blocks resident per SM (71 KB of shared memory each) the bulk
 // copies of one block's item overlap the compute and stores of the others.
 template <class Map, class Op>
-__global__ void __launch_bounds__(kDmBlock) k_dm_engine(DevMemBulk mem, Map map, DmGeom g, Op op) {
+__global__ void __launch_bounds__(kDmBlock, kDmMinBlocks) k_dm_engine(DevMemBulk mem, Map map, DmGeom g, Op op) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw);
     DmPos* pd = reinterpret_cast<DmPos*>(smem_raw + 16);
@@ -803,16 +814,15 @@ __global__ void __launch_bounds__(kDmBlock) k_dm_engine(DevMemBulk mem, Map map,
             __syncthreads();                               // everyone has read the flags
             continue;
         }
-        if (tid < 32) {                                     // warp 0 arms the barrier and issues the loads
-            if (tid == 0) {
-                unsigned bytes = 0;
-                for (unsigned t = 0; t < npos; ++t) bytes += pd[t].bytes;
-                mbar_arrive_expect(bar, bytes);
-            }
-            __syncwarp();
-            fence_proxy_async();
-            dm_bulk_loads(mem, map, g, pd, vb, bar, tid, 32u);
+        if (tid == 0) {                                     // arm the barrier with the item's bytes
+            unsigned bytes = 0;
+            for (unsigned t = 0; t < npos; ++t) bytes += pd[t].bytes;
+            mbar_arrive_expect(bar, bytes);
         }
+        // every thread issues its share of the bulk loads (a warp issues them one after
+        // another, so one issuing warp would cap the block's copy rate)
+        fence_proxy_async();
+        dm_bulk_loads(mem, map, g, pd, vb, bar, tid, nthr);
         const unsigned long long fix0 = dm_pass_mask<Map>(pd, npos, 0);
         const unsigned long long fix1 = dm_pass_mask<Map>(pd, npos, 1);
         const unsigned long long mirr = dm_pass_mask<Map>(pd, npos, 2);
@@ -831,12 +841,10 @@ __global__ void __launch_bounds__(kDmBlock) k_dm_engine(DevMemBulk mem, Map map,
         }
         fence_proxy_async();
         __syncthreads();
-        if (tid < 32) {
-            dm_bulk_stores(mem, map, g, pd, vb, tid, 32u);
-            bulk_commit();
-        }
+        dm_bulk_stores(mem, map, g, pd, vb, tid, nthr);
+        bulk_commit();
         if (mirr) dm_mirror_stores(mem, map, g, pd, vb, mirr, tid, nthr);
-        if (tid < 32) bulk_wait_read();                     // the staged block may be refilled
+        bulk_wait_read();                                   // the staged block may be refilled
         __syncthreads();
     }
     if (!ok) {
@@ -844,7 +852,7 @@ __global__ void __launch_bounds__(kDmBlock) k_dm_engine(DevMemBulk mem, Map map,
         for (unsigned long long i = 0; i < kDmWaitLimit && !mbar_try_wait(bar, parity); ++i) {
         }
     }
-    if (tid < 32) bulk_wait_all();
+    bulk_wait_all();
 }
 #endif
 
