@@ -43,6 +43,11 @@ inline PhaseGeom phase_geometry(unsigned n, unsigned ls_max) {
 struct GateFactor1 {
     unsigned q;
     double2 ph1;
+    // can any element of the S x S item at (R, C) change?  (bit q is constant over the item
+    // when q >= log2 S)
+    ORKAN_HD bool item_active(idx_t R, idx_t C, unsigned ls) const {
+        return q < ls || (((R ^ C) >> q) & 1u);
+    }
     ORKAN_HD bool factor(idx_t r, idx_t c, double2* f) const {
         const unsigned br = (unsigned)(r >> q) & 1u, bc = (unsigned)(c >> q) & 1u;
         if (br == bc) return false;
@@ -57,6 +62,12 @@ struct GateFactor1 {
 struct GateFactorCtrl {
     unsigned long long mask;
     double2 ph;
+    // the mask bits at or above log2 S are constant over the item: rows (columns) can meet
+    // the mask only when R (C) has all of them
+    ORKAN_HD bool item_active(idx_t R, idx_t C, unsigned ls) const {
+        const unsigned long long hi = mask & ~((1ull << ls) - 1ull);
+        return (((unsigned long long)R & hi) == hi) || (((unsigned long long)C & hi) == hi);
+    }
     ORKAN_HD bool factor(idx_t r, idx_t c, double2* f) const {
         const bool br = ((unsigned long long)r & mask) == mask, bc = ((unsigned long long)c & mask) == mask;
         if (br == bc) return false;
@@ -71,6 +82,7 @@ struct GateFactor {
     unsigned k;
     unsigned q[3];
     double2 phase[8];
+    ORKAN_HD bool item_active(idx_t, idx_t, unsigned) const { return true; }
     ORKAN_HD unsigned local(idx_t x) const {
         unsigned l = 0;
         for (unsigned j = 0; j < k; ++j) l = (l << 1) | (unsigned)((x >> q[j]) & 1u);
@@ -94,6 +106,7 @@ struct GateFactor {
 template <class MemR2>
 struct TableFactor {
     MemR2 tab;
+    ORKAN_HD bool item_active(idx_t, idx_t, unsigned) const { return true; }
     ORKAN_HD bool factor(idx_t r, idx_t c, double2* f) const {
         const double2 pr = tab.ld(r), pc = tab.ld(c);
         f->x = pr.x * pc.x + pr.y * pc.y;
@@ -127,6 +140,7 @@ ORKAN_HD void dm_phase_item(const Mem& mem, const Map& map, const PhaseGeom& g, 
     tri_unrank_fast(w, &u, &v);
     const unsigned ls = g.ls, S = 1u << ls;
     const idx_t R = u << ls, C = v << ls;
+    if (!fac.item_active(R, C, ls)) return;
     const unsigned total = S * S;
     const bool diag = (u == v);
     const idx_t base = map.at(R, C);
