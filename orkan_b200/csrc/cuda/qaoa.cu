@@ -8,6 +8,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -646,10 +647,10 @@ int orkan_qaoa_tune(orkan_qaoa_t* b, const double* gammas, const double* betas, 
                 bytes += (size_t(1) << nq) * 16;
                 sel.push_back(i);
             }
-        float best = 1e30f;
-        QaoaCfg bestc = b->cfg[nq];
-        // chunks from the smallest that keeps the high pass possible (2C >= n) up to 2^13;
-        // a chunk of at least n qubits is the full pass, where only n matters
+        // candidates: chunks from the smallest that keeps the high pass possible (2C >= n)
+        // up to 2^13 (a chunk of at least n qubits is the full pass, where only n matters),
+        // thread counts that give a register stage 1..4 sets per thread, ring depth 1 or 2
+        std::vector<QaoaCfg> cands;
         const unsigned c_lo = std::min(kQaoaMaxC, std::max(nq <= 11 ? nq : 11u, (nq + 1) / 2));
         for (unsigned Cc = c_lo; Cc <= kQaoaMaxC; ++Cc) {
             const unsigned lc = Cc >= nq ? nq : Cc;
@@ -657,24 +658,52 @@ int orkan_qaoa_tune(orkan_qaoa_t* b, const double* gammas, const double* betas, 
                 const unsigned sets = (1u << lc) / 16;       // 16-amplitude sets of a register stage
                 if (tt > std::max(128u, sets) || tt * 4 < sets) continue;
                 for (unsigned rg : {1u, 2u}) {
-                    const bool bytes_cost = grp.second;
-                    const size_t smem = bytes_cost ? qaoa_smem_bytes<uint8_t>(lc, tt, rg) : qaoa_smem_bytes<double>(lc, tt, rg);
-                    if (smem > kSmemLimit) continue;
-                    b->cfg[nq] = QaoaCfg{Cc, tt, rg};
-                    Plan pl = make_plan(b, sel);
-                    if (upload_plan(b, pl)) { cudaGetLastError(); continue; }
-                    if (enqueue_kernels(b, pl, b->cap)) { cudaGetLastError(); continue; }   // warm-up
-                    cudaEventRecord(e0, b->cap);
-                    bool ok = true;
-                    for (int r = 0; r < 3 && ok; ++r) ok = enqueue_kernels(b, pl, b->cap) == 0;
-                    cudaEventRecord(e1, b->cap);
-                    if (!ok || cudaEventSynchronize(e1) != cudaSuccess) { cudaGetLastError(); continue; }
-                    float ms = 0.f;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                    if (ms < best) { best = ms; bestc = b->cfg[nq]; }
+                    const size_t smem = grp.second ? qaoa_smem_bytes<uint8_t>(lc, tt, rg) : qaoa_smem_bytes<double>(lc, tt, rg);
+                    if (smem <= kSmemLimit) cands.push_back(QaoaCfg{Cc, tt, rg});
                 }
             }
             if (Cc >= nq) break;                            // a full pass: larger chunks change nothing
+        }
+        // three rounds over the candidates, interleaved, each timing three runs of the
+        // sample; a candidate's figure is its median round, so that a drift of the clocks
+        // or a single disturbed round does not decide.  The rx coefficients depend on the
+        // chunk and are staged for each candidate.
+        constexpr int kRounds = 3;
+        std::vector<std::array<float, kRounds>> times(cands.size());
+        std::vector<bool> usable(cands.size(), true);
+        for (int round = 0; round < kRounds; ++round) {
+            for (size_t ci = 0; ci < cands.size(); ++ci) {
+                if (!usable[ci]) continue;
+                b->cfg[nq] = cands[ci];
+                stage_angles(b, gammas, betas);
+                Plan pl = make_plan(b, sel);
+                bool ok = upload_plan(b, pl) == 0 &&
+                          cudaMemcpyAsync(b->d_rx, b->h_rx, np * sizeof(QaoaRx), cudaMemcpyHostToDevice, b->cap) == cudaSuccess;
+                if (ok && round == 0) ok = enqueue_kernels(b, pl, b->cap) == 0;       // warm-up
+                if (ok) ok = cudaEventRecord(e0, b->cap) == cudaSuccess;
+                for (int r = 0; r < 3 && ok; ++r) ok = enqueue_kernels(b, pl, b->cap) == 0;
+                if (ok) ok = cudaEventRecord(e1, b->cap) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
+                float ms = 0.f;
+                if (ok) ok = cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+                if (!ok) {
+                    cudaGetLastError();
+                    cudaStreamSynchronize(b->cap);
+                    usable[ci] = false;
+                    continue;
+                }
+                times[ci][round] = ms;
+            }
+        }
+        float best = 1e30f;
+        QaoaCfg bestc = default_cfg(nq);
+        for (size_t ci = 0; ci < cands.size(); ++ci) {
+            if (!usable[ci]) continue;
+            auto t = times[ci];
+            std::sort(t.begin(), t.end());
+            if (t[kRounds / 2] < best) {
+                best = t[kRounds / 2];
+                bestc = cands[ci];
+            }
         }
         b->cfg[nq] = bestc;
         char line[512];
