@@ -434,68 +434,91 @@ def batched_cpu_baseline(ns, edges, g, b, budget_s):
                       f"amplitude-calls, OpenMP threads = {cores}"}
 
 
-def batched_leg(args, ork, clocks_cls, local):
+def batched_leg(args, ork, clocks_cls, local, dist=None, rank=0, world=1):
+    """The batched QAOA leg.  With N ranks the instances are partitioned by work
+    (`shard_instances`), every rank evaluates its share on its GPU and the whole batch's
+    means are gathered on every rank (one all-reduce of `count` doubles); the device time
+    is the slowest rank's, the e2e time includes the gather."""
     import numpy as np
     import torch
-    from orkan_b200.batch import QaoaBatch
+    from orkan_b200.batch import ShardedQaoaBatch
     count, p = args.batch_instances, 4
     ns, edges, g, b = qaoa_batch_workload(count, p)
-    bt = QaoaBatch(ork, ns, edges, None, p)
+    sh = ShardedQaoaBatch(ork, ns, edges, None, p, rank=rank, world=world)
+    bt = sh.local
     t0 = time.perf_counter()
-    bt.tune(g, b, None)
+    sh.tune(g, b, None)
     tune_s = time.perf_counter() - t0
     for _ in range(max(3, args.warmup)):
-        bt.run(g, b)
+        sh.run(g, b)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     clk = clocks_cls(local)
     clk.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     steps = max(1, args.steps)
     e0.record()
-    w0 = time.perf_counter()
     for _ in range(steps):
-        means = bt.run(g, b)                # public API: host angles in, host means out
+        local_means = sh.run(g, b)          # public API: host angles in, host means out
     e1.record()
     torch.cuda.synchronize()
-    wall = (time.perf_counter() - w0) / steps
-    ms = e0.elapsed_time(e1) / steps
+    ms = reduce_max(e0.elapsed_time(e1) / steps, dist, "cuda")
     clocks = clk.stop()
-    waves, launches = bt.stats()
+    # end to end: the same runs plus the gather of the whole batch's means on every rank
+    if dist:
+        dist.barrier()
+    w0 = time.perf_counter()
+    for _ in range(steps):
+        means = sh.gather(sh.run(g, b), dist, "cuda")
+    wall = reduce_max((time.perf_counter() - w0) / steps, dist, "cuda")
+    waves, launches = bt.stats() if bt is not None else (0, 0)
     amps = float(sum(2.0 ** int(n) for n in ns))
     per_amp = 16 + (p - 1) * 32 + 16 + (p + 1) * 1          # state traffic of the p + 1 passes, byte costs
     achieved = amps * per_amp / (ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
-    # every instance of a 64-instance sample against the per-call plain path of this library
-    rng = np.random.default_rng(5)
-    sample = rng.choice(count, 64, replace=False)
-    errs, t_plain, amps_plain = [], 0.0, 0.0
-    for i in sample:
-        cost = bt.cost_vector(int(i))
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        m = plain_qaoa_mean(ork, int(ns[i]), cost, g[i], b[i])
-        t_plain += time.perf_counter() - t1
-        amps_plain += 2.0 ** int(ns[i])
-        errs.append(abs(m - means[i]))
-    plain_evals = count / (t_plain / amps_plain * amps)
-    configs = {int(n): list(bt.config(int(n))) for n in sorted(set(int(x) for x in ns))}
-    bt.close()
-    cpu = batched_cpu_baseline(ns, edges, g, b, args.cpu_seconds) if not args.no_cpu_baseline else None
-    return {"metric": "batched evals/s", "value": count / (ms * 1e-3), "unit": "evals/s",
-            "e2e": {"value": count / wall, "unit": "evals/s", "h2d_bytes_per_step": count * p * (8 + 24),
-                    "d2h_bytes_per_step": count * 8},
-            "ms_per_batch": ms, "dtype": "f64",
-            "config": {"workload": f"{count} QAOA MaxCut instances, qubits uniform 16..24, random 3-regular graphs "
-                                   f"(one vertex of degree 2 when n is odd), p = {p}, gamma U[0, pi], beta U[0, pi/2]",
-                       "instances": count, "p": p, "waves": waves, "launches_per_run": launches,
-                       "tuned": configs, "tune_seconds": tune_s,
-                       "l2": "state vectors 1 MiB..256 MiB per instance, 62 GB per wave: larger than L2"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
-                         "frac": achieved / peak, "algorithmic_bytes_per_amplitude": per_amp},
-            "checked_vs_plain": {"instances": len(errs), "max_abs_err": max(errs), "tolerance": 1e-12},
-            "plain_per_call_gpu_evals_per_s": plain_evals,
-            "speedup_vs_plain_per_call": (count / (ms * 1e-3)) / plain_evals,
-            "cpu_baseline": cpu, "clocks": clocks}
+    configs = ({int(n): list(bt.config(int(n))) for n in sorted(set(int(ns[i]) for i in sh.idx))}
+               if bt is not None else {})
+    line = None
+    if rank == 0:
+        # every instance of a 64-instance sample of this rank's share against the per-call
+        # plain path of this library (the gathered vector holds the batch's means)
+        rng = np.random.default_rng(5)
+        pick = rng.choice(len(sh.idx), min(64, len(sh.idx)), replace=False)
+        errs, t_plain, amps_plain = [], 0.0, 0.0
+        for j in pick:
+            i = int(sh.idx[j])
+            cost = bt.cost_vector(int(j))
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            m = plain_qaoa_mean(ork, int(ns[i]), cost, g[i], b[i])
+            t_plain += time.perf_counter() - t1
+            amps_plain += 2.0 ** int(ns[i])
+            errs.append(max(abs(m - means[i]), abs(m - local_means[j])))
+        plain_evals = count / (t_plain / amps_plain * amps)
+        cpu = (batched_cpu_baseline(ns, edges, g, b, args.cpu_seconds)
+               if not args.no_cpu_baseline and world == 1 else None)
+        line = {"metric": "batched evals/s", "value": count / (ms * 1e-3), "unit": "evals/s",
+                "e2e": {"value": count / wall, "unit": "evals/s", "h2d_bytes_per_step": count * p * (8 + 24),
+                        "d2h_bytes_per_step": count * 8},
+                "ms_per_batch": ms, "dtype": "f64",
+                "config": {"workload": f"{count} QAOA MaxCut instances, qubits uniform 16..24, random 3-regular "
+                                       f"graphs (one vertex of degree 2 when n is odd), p = {p}, gamma U[0, pi], "
+                                       f"beta U[0, pi/2]",
+                           "instances": count, "p": p, "ranks": world, "instances_rank0": len(sh.idx),
+                           "waves": waves, "launches_per_run": launches, "tuned": configs,
+                           "tune_seconds": tune_s, "per_rank_fields": "waves, launches_per_run and tuned "
+                                                                      "describe rank 0's share",
+                           "l2": "state vectors 1 MiB..256 MiB per instance, 62 GB per wave: larger than L2"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak * world, "peak_source": peak_kind,
+                             "unit": "GB/s", "frac": achieved / (peak * world),
+                             "algorithmic_bytes_per_amplitude": per_amp},
+                "checked_vs_plain": {"instances": len(errs), "max_abs_err": max(errs), "tolerance": 1e-12},
+                "plain_per_call_gpu_evals_per_s": plain_evals,
+                "speedup_vs_plain_per_call": (count / (ms * 1e-3)) / plain_evals,
+                "cpu_baseline": cpu, "clocks": clocks}
+    sh.close()
+    return line
 
 
 # ---------------------------------------------------------------------------------------
@@ -744,8 +767,8 @@ def run_gpu(args):
     batched = surrogate = noisy = channels = None
     if rank == 0 and world == 1 and args.channel_qubits > 0:
         channels = channels_leg(args, ork, ClockSampler, local)
-    if rank == 0 and world == 1 and args.batch_instances > 0:
-        batched = batched_leg(args, ork, ClockSampler, local)
+    if args.batch_instances > 0:             # every rank: the batch is sharded over the ranks
+        batched = batched_leg(args, ork, ClockSampler, local, dist, rank, world)
     if rank == 0 and world == 1 and args.surrogate_pairs > 0:
         surrogate = surrogate_leg(args, ork)
     if rank == 0 and world == 1 and args.noisy_pairs > 0:

@@ -116,6 +116,84 @@ class QaoaBatch:
             pass
 
 
+def shard_instances(n_qubits, world: int) -> list[np.ndarray]:
+    """Partition instances over `world` ranks by work (2^n amplitude-passes each): instances
+    in descending order of n (index order among equals), each to the rank with the least
+    work so far (lowest rank on ties).  Returns each rank's instance indices, ascending.
+    Deterministic, so every rank computes the same partition without communication."""
+    n = np.asarray(n_qubits, dtype=np.int64)
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    order = sorted(range(len(n)), key=lambda i: (-int(n[i]), i))
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += 1 << int(n[i])
+    return [np.array(sorted(p), dtype=np.int64) for p in parts]
+
+
+def scatter_means(count: int, idx, local_means) -> np.ndarray:
+    """A full-length vector holding this rank's means at their instance indices and 0.0
+    elsewhere; the sum of all ranks' vectors is the whole batch (x + 0.0 == x exactly)."""
+    out = np.zeros(count, dtype=np.float64)
+    if len(idx):
+        out[np.asarray(idx)] = np.asarray(local_means, dtype=np.float64)
+    return out
+
+
+def gather_means(count: int, idx, local_means, dist=None, device="cpu") -> np.ndarray:
+    """Every rank's means in instance order, on every rank (one all-reduce of `count`
+    doubles over the process group; the local vector alone without one)."""
+    part = scatter_means(count, idx, local_means)
+    if dist is None:
+        return part
+    import torch
+    t = torch.from_numpy(part).to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.cpu().numpy()
+
+
+class ShardedQaoaBatch:
+    """This rank's share of a QAOA batch spread over `world` ranks (one GPU each): the
+    instances of `shard_instances(n_qubits, world)[rank]` in a local QaoaBatch.  `run`
+    evaluates the local share; `gather` assembles the whole batch's means on every rank.
+    Instances are independent, so the only exchange is that final gather."""
+
+    def __init__(self, ork, n_qubits, edges, weights=None, p: int = 1, rank: int = 0, world: int = 1, **kw):
+        self.count, self.p = len(n_qubits), int(p)
+        self.idx = shard_instances(n_qubits, world)[rank]
+        sel = [int(i) for i in self.idx]
+        self.local = None
+        if sel:
+            self.local = QaoaBatch(ork, [int(n_qubits[i]) for i in sel], [edges[i] for i in sel],
+                                   None if weights is None else [weights[i] for i in sel], p, **kw)
+
+    def _local_angles(self, gammas, betas):
+        g = np.asarray(gammas, dtype=np.float64).reshape(self.count, self.p)[self.idx]
+        b = np.asarray(betas, dtype=np.float64).reshape(self.count, self.p)[self.idx]
+        return g, b
+
+    def tune(self, gammas, betas, cache_path: str | None = None) -> None:
+        if self.local is not None:
+            self.local.tune(*self._local_angles(gammas, betas), cache_path)
+
+    def run(self, gammas, betas) -> np.ndarray:
+        """Means of this rank's instances (in the order of `self.idx`)."""
+        if self.local is None:
+            return np.zeros(0)
+        return self.local.run(*self._local_angles(gammas, betas))
+
+    def gather(self, local_means, dist=None, device="cpu") -> np.ndarray:
+        return gather_means(self.count, self.idx, local_means, dist, device)
+
+    def close(self) -> None:
+        if self.local is not None:
+            self.local.close()
+            self.local = None
+
+
 def random_regular_graph(n: int, d: int, rng) -> list[tuple[int, int]]:
     """A uniformly drawn simple d-regular graph on n vertices (configuration model with
     rejection of loops and multi-edges).  When n * d is odd no such graph exists; then one

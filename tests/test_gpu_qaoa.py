@@ -174,3 +174,29 @@ def test_regular_batch_every_instance_vs_plain_path(ork):
         for i in range(count):
             cost = bt.cost_vector(i)
             assert abs(means[i] - plain_mean(ork, int(ns[i]), cost, g[i], b[i])) < TOL, f"instance {i}"
+
+
+def test_sharded_batch_matches_the_whole_batch(ork):
+    """The batch split over three ranks (here three shards on one GPU, no process group):
+    each shard's means, scattered to their instance indices and summed, equal the whole
+    batch's."""
+    from orkan_b200.batch import ShardedQaoaBatch, scatter_means
+    rng = np.random.default_rng(19)
+    ns = [int(x) for x in rng.integers(10, 19, 30)]
+    p = 3
+    edges, _ = graphs_for(ns, rng)
+    g, b = angles(len(ns), p, rng)
+    with QaoaBatch(ork, ns, edges, None, p) as whole:
+        want = whole.run(g, b)
+    total = np.zeros(len(ns))
+    seen = []
+    for rank in range(3):
+        sh = ShardedQaoaBatch(ork, ns, edges, None, p, rank=rank, world=3)
+        loc = sh.run(g, b)
+        assert len(loc) == len(sh.idx) > 0
+        total += scatter_means(len(ns), sh.idx, loc)
+        assert np.array_equal(sh.gather(loc), scatter_means(len(ns), sh.idx, loc))
+        seen.extend(sh.idx.tolist())
+        sh.close()
+    assert sorted(seen) == list(range(len(ns)))
+    assert np.abs(total - want).max() < TOL
