@@ -20,6 +20,7 @@
 #ifndef ORKAN_CU_H
 #define ORKAN_CU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -117,6 +118,23 @@ unsigned orkan_cu_engine_status(void);
 
 /* Number of kernels this library has launched in this process (all devices). */
 unsigned long long orkan_cu_launch_count(void);
+
+/* ---- sample-matrix building blocks (sample_matrix, include/orkan_sample.h; the reference
+ * specifies the operation in docs/SAMPLE_MATRIX.md and has no implementation) ---------- */
+
+/* acc = w x (first != 0) or acc += w x over len amplitudes (w = w_re + i w_im). */
+int orkan_cu_lincomb(void *acc, const void *x, double w_re, double w_im, unsigned long long len, int first,
+                     void *stream);
+
+/* Bytes of device scratch orkan_cu_sm_block needs (fixed; about 2 MiB). */
+size_t orkan_cu_sm_scratch_bytes(void);
+
+/* out[i + j bi] = sum_x conj(phi_i[i len + x]) obs[x] phi_j[j len + x] for i < bi, j < bj
+ * (1 <= bi, bj <= 16; columns of len amplitudes, consecutive).  The sum over x runs in a
+ * fixed partition and order that depend only on len, so an entry is the same bit for bit
+ * whatever block it is computed in. */
+int orkan_cu_sm_block(const void *phi_i, unsigned bi, const void *phi_j, unsigned bj, unsigned long long len,
+                      const double *obs, void *out, void *scratch, void *stream);
 
 #ifdef __cplusplus
 }

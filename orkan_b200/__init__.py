@@ -36,6 +36,14 @@ class SuperopT(C.Structure):
     _fields_ = [("n_qubits", C.c_ubyte), ("data", C.c_void_p)]
 
 
+QOP = C.CFUNCTYPE(None, C.POINTER(StateT))     # qop_t of include/state.h
+
+
+class SmChannel(C.Structure):
+    """sm_channel_t of include/orkan_sample.h."""
+    _fields_ = [("n_ops", C.c_uint), ("ops", C.POINTER(QOP)), ("weights", C.c_void_p)]
+
+
 class OrkanError(RuntimeError):
     pass
 
@@ -107,6 +115,8 @@ class Orkan:
         L.orkan_launch_count.restype = C.c_ulonglong
         L.orkan_debug_fail_allocs.argtypes = [C.c_int]
         L.orkan_cu_launch_count.restype = C.c_ulonglong
+        L.sample_matrix.argtypes = [P, vp, C.POINTER(SmChannel), C.c_uint, C.c_uint, C.c_size_t, vp]
+        L.sample_matrix.restype = None
 
     # ---- states ------------------------------------------------------------------
     def state(self, kind: str, n: int, storage: np.ndarray | None = None) -> StateT:
@@ -203,6 +213,30 @@ class Orkan:
     def two_from_mat(self, s: StateT, q1: int, q2: int, mat_colmajor: np.ndarray) -> None:
         arr = np.ascontiguousarray(mat_colmajor, dtype=np.complex128)
         self.lib.two_from_mat(C.byref(s), int(q1), int(q2), arr.ctypes.data)
+
+    def sample_matrix(self, iota: StateT, obs, channels, at: int, workspace_bytes: int) -> np.ndarray:
+        """S^(at) of include/orkan_sample.h.  channels: a list of (ops, weights), ops Python
+        callables op(state: StateT) that apply gates to the state in place, weights a complex
+        sequence (None allowed at `at`).  iota is consumed (it holds the prefix state on
+        return).  Returns the K x K complex matrix."""
+        keep = []
+        arr = (SmChannel * len(channels))()
+        for k, (ops, weights) in enumerate(channels):
+            cbs = [QOP(lambda sp, f=f: f(sp.contents)) for f in ops]
+            table = (QOP * len(cbs))(*cbs)
+            keep += cbs + [table]
+            wptr = None
+            if weights is not None:
+                w = np.ascontiguousarray(weights, dtype=np.complex128)
+                keep.append(w)
+                wptr = w.ctypes.data
+            arr[k] = SmChannel(len(cbs), C.cast(table, C.POINTER(QOP)), wptr)
+        K = len(channels[at][0])
+        out = np.zeros((K, K), dtype=np.complex128, order="F")
+        ob = obs if isinstance(obs, int) else np.ascontiguousarray(obs, dtype=np.float64)
+        self.lib.sample_matrix(C.byref(iota), ob if isinstance(ob, int) else ob.ctypes.data, arr, len(channels),
+                               int(at), int(workspace_bytes), out.ctypes.data)
+        return out
 
     def set_stream(self, handle: int | None) -> None:
         self.lib.orkan_set_stream(handle)

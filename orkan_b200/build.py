@@ -28,8 +28,8 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
 CC_FLAGS = ["-std=gnu17", "-O2", "-fPIC", "-Wall", "-Wno-unused-function", "-I" + INCLUDE,
             "-I" + os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["orkan_cu.cu", "scratch.cu", "noalloc.cu", "qaoa.cu", "mlp.cu"]
-C_SOURCES = ["runtime.c", "state.c", "gate.c", "channel.c", "meas.c", "circ.c"]
+CU_SOURCES = ["orkan_cu.cu", "scratch.cu", "noalloc.cu", "qaoa.cu", "mlp.cu", "sample.cu"]
+C_SOURCES = ["runtime.c", "state.c", "gate.c", "channel.c", "meas.c", "circ.c", "sample.c"]
 LIBS = {5: "liborkan_b200.so", 3: "liborkan_b200_t3.so"}
 
 
