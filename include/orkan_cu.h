@@ -79,6 +79,13 @@ int orkan_cu_dm_phase(int layout, unsigned log_tile, void *rho, unsigned n, unsi
 int orkan_cu_dm_superop1(int layout, unsigned log_tile, void *rho, unsigned n, unsigned target,
                          const double *sop, void *stream);
 
+/* 2-qubit superoperator on (q0, q1): sop = 16 x 16 row-major complex over vec(rho_4x4) with
+ * vec index 4 * row + column and local index 2 * bit(q0) + bit(q1).  No counterpart in the
+ * reference, whose channel_1q takes 1-local superoperators only (src/channel/channel.c:67-85)
+ * although kraus_to_superop builds them for any qubit count (channel.c:21-50). */
+int orkan_cu_dm_superop2(int layout, unsigned log_tile, void *rho, unsigned n, unsigned q0, unsigned q1,
+                         const double *sop, void *stream);
+
 /* exp_diag with a DEVICE diag array of 2^n doubles.  Replaces exp_diag_pure /
  * exp_diag_packed / exp_diag_tiled (reference src/circ/circ_pure.c:21-33,
  * circ_packed.c:28-71, circ_tiled.c:25-105).  t == 0 is a no-op. */

@@ -6,6 +6,7 @@
 #define ORKAN_DEV_H
 
 #include "state.h"
+#include "channel.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -27,6 +28,12 @@ void orkan_sync(void);
  * orkan_state_upload does not take ownership of host (compare state_init). */
 int orkan_state_upload(state_t *state, const cplx_t *host);
 int orkan_state_download(const state_t *state, cplx_t *host);
+
+/* 2-qubit channel on a density matrix: sop from kraus_to_superop of 2-qubit Kraus operators
+ * (16 x 16), local index 2 * bit(q0) + bit(q1).  The reference's channel_1q takes 1-local
+ * superoperators only; this is its 2-local counterpart, with the same validation behaviour
+ * ("orkan: channel: <msg>" and exit). */
+void channel_2q(state_t *state, const superop_t *sop, qubit_t q0, qubit_t q1);
 
 /* Kernels launched by the library so far in this process. */
 unsigned long long orkan_launch_count(void);

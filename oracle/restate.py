@@ -325,6 +325,21 @@ def apply_superop1(rho: np.ndarray, sop: np.ndarray, q: int) -> np.ndarray:
     return np.ascontiguousarray(t).reshape(rho.shape)
 
 
+def apply_superop2(rho: np.ndarray, sop: np.ndarray, q0: int, q1: int) -> np.ndarray:
+    """vec(rho_4x4)' = S vec(rho_4x4) for every 4x4 block of qubits (q0, q1): vec index
+    4 * row + column, local index 2 * bit(q0) + bit(q1).  The library's own 2-qubit channel
+    (no reference counterpart; kraus_to_superop builds the 16 x 16 superoperator,
+    src/channel/channel.c:21-50), checked against the Kraus sum in the tests."""
+    n = int(rho.shape[0]).bit_length() - 1
+    t = rho.reshape([2] * (2 * n))
+    axes = [n - 1 - q0, n - 1 - q1, 2 * n - 1 - q0, 2 * n - 1 - q1]
+    t = np.moveaxis(t, axes, [0, 1, 2, 3])
+    shp = t.shape
+    t = (sop @ t.reshape(16, -1)).reshape(shp)
+    t = np.moveaxis(t, [0, 1, 2, 3], axes)
+    return np.ascontiguousarray(t).reshape(rho.shape)
+
+
 def depolarizing_kraus(p: float):
     """p/4 form of the reference tests (test/channel/test_channel_tiled.c:38-45)."""
     a, b = np.sqrt(1.0 - 3.0 * p / 4.0), np.sqrt(p / 4.0)

@@ -103,6 +103,7 @@ class Orkan:
         L.kraus_to_superop.argtypes = [C.POINTER(KrausT)]
         L.kraus_to_superop.restype = SuperopT
         L.channel_1q.argtypes = [P, C.POINTER(SuperopT), C.c_ubyte]
+        L.channel_2q.argtypes = [P, C.POINTER(SuperopT), C.c_ubyte, C.c_ubyte]
         L.single_from_mat.argtypes = [P, C.c_ubyte, vp]
         L.two_from_mat.argtypes = [P, C.c_ubyte, C.c_ubyte, vp]
         L.orkan_log_tile_dim.restype = C.c_int
@@ -205,6 +206,12 @@ class Orkan:
         arr = np.ascontiguousarray(np.asarray(sop).reshape(-1), dtype=np.complex128)
         so = SuperopT(1, arr.ctypes.data)
         self.lib.channel_1q(C.byref(s), C.byref(so), int(q))
+
+    def channel_2q(self, s: StateT, sop: np.ndarray, q0: int, q1: int) -> None:
+        """2-qubit channel (16 x 16 superoperator, local index 2 bit(q0) + bit(q1))."""
+        arr = np.ascontiguousarray(np.asarray(sop).reshape(-1), dtype=np.complex128)
+        so = SuperopT(2, arr.ctypes.data)
+        self.lib.channel_2q(C.byref(s), C.byref(so), int(q0), int(q1))
 
     def single_from_mat(self, s: StateT, q: int, mat_colmajor: np.ndarray) -> None:
         arr = np.ascontiguousarray(mat_colmajor, dtype=np.complex128)

@@ -508,6 +508,38 @@ struct OpSuper1 {
     }
 };
 
+// 2-qubit superoperator (row-major s[16 * m + j], vec index 4 * row + column of the 4 x 4
+// block over the two gate qubits, local index 2 * bit(q0) + bit(q1)) on 4 x 4 groups.
+struct OpSuper2 {
+    double2 s[256];
+    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr, unsigned = 3u) const {
+        const unsigned P = g.P(), lq = g.ls + g.h - 2;
+        unsigned asc[2] = {g.vbit[0] < g.vbit[1] ? g.vbit[0] : g.vbit[1],
+                           g.vbit[0] < g.vbit[1] ? g.vbit[1] : g.vbit[0]};
+        const unsigned groups = 1u << (2 * lq);
+        for (unsigned t = tid; t < groups; t += nthr) {
+            const unsigned rb = (unsigned)insert0_sorted(t >> lq, asc, 2);
+            const unsigned cb = (unsigned)insert0_sorted(t & ((1u << lq) - 1), asc, 2);
+            unsigned ri[4], ci[4];
+            for (unsigned l = 0; l < 4; ++l) {
+                ri[l] = dm_set_local(rb, l, g.vbit, 2);
+                ci[l] = dm_set_local(cb, l, g.vbit, 2);
+            }
+            // the group's 16 elements belong to this thread alone: all read, then written
+            double2 x[16];
+            for (unsigned r = 0; r < 4; ++r)
+                for (unsigned c = 0; c < 4; ++c) x[4 * r + c] = vb[ri[r] * P + ci[c]];
+#pragma unroll 1
+            for (unsigned m = 0; m < 16; ++m) {
+                double2 acc = c2(0.0, 0.0);
+#pragma unroll
+                for (unsigned j = 0; j < 16; ++j) acc = cadd(acc, cmul(s[16 * m + j], x[j]));
+                vb[ri[m >> 2] * P + ci[m & 3]] = acc;
+            }
+        }
+    }
+};
+
 // Monomial gate U|x> with an involutive permutation (X, Y, CX, CY, SWAP, CCX ...):
 // (U psi)[y] = phase[y] * psi[src[y]] on the local index, src[src[y]] == y.
 // Element pairs (y, z) <-> (src y, src z) are 2-cycles; the thread owning the
@@ -701,6 +733,15 @@ inline void dm_orient(OpMonomial& op, bool transposed) {
     op.p0 = cconj(op.p0);
     op.p1 = cconj(op.p1);
 }
+// vec(rho^T) holds element (i, j) at 4 j + i: rows and columns of the superoperator are
+// permuted by 4 i + j <-> 4 j + i.
+inline void dm_orient(OpSuper2& op, bool transposed) {
+    if (!transposed) return;
+    double2 t[256];
+    for (unsigned m = 0; m < 16; ++m)
+        for (unsigned j = 0; j < 16; ++j) t[16 * m + j] = op.s[16 * (((m & 3) << 2) | (m >> 2)) + (((j & 3) << 2) | (j >> 2))];
+    for (unsigned i = 0; i < 256; ++i) op.s[i] = t[i];
+}
 inline void dm_orient(OpSuper1& op, bool transposed) {
     if (!transposed) return;
     const unsigned perm[4] = {0, 2, 1, 3};
@@ -786,13 +827,15 @@ __device__ __forceinline__ bool dm_wait_stage(unsigned long long* bar, unsigned 
 
 // Blocks per SM the register budget is held to: three blocks with a 64 x 64 staged block
 // fill the shared memory, and the bulk copies of one overlap the compute of the others.
-constexpr int kDmMinBlocks = 3;
+// The 2-qubit superoperator holds a whole 4 x 4 group in registers and gets two.
+template <class Op> struct DmMinBlocks { static constexpr int value = 3; };
+template <> struct DmMinBlocks<OpSuper2> { static constexpr int value = 2; };
 
 // Persistent engine: block b handles items b, b + G, b + 2G, ...  One item at a time per
 // block; with up to three blocks resident per SM (71 KB of shared memory each) the bulk
 // copies of one block's item overlap the compute and stores of the others.
 template <class Map, class Op>
-__global__ void __launch_bounds__(kDmBlock, kDmMinBlocks) k_dm_engine(DevMemBulk mem, Map map, DmGeom g, Op op) {
+__global__ void __launch_bounds__(kDmBlock, DmMinBlocks<Op>::value) k_dm_engine(DevMemBulk mem, Map map, DmGeom g, Op op) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw);
     DmPos* pd = reinterpret_cast<DmPos*>(smem_raw + 16);

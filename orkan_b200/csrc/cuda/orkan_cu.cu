@@ -277,6 +277,18 @@ int orkan_cu_dm_superop1(int layout, unsigned log_tile, void* rho, unsigned n, u
     return launch_engine_map(layout, log_tile, rho, n, g, op, as_stream(stream));
 }
 
+int orkan_cu_dm_superop2(int layout, unsigned log_tile, void* rho, unsigned n, unsigned q0, unsigned q1,
+                         const double* sop, void* stream) {
+    if (!rho || !sop || !layout_ok(layout, log_tile) || q0 >= n || q1 >= n || q0 == q1 || n > 40)
+        return (int)cudaErrorInvalidValue;
+    OpSuper2 op;
+    for (unsigned i = 0; i < 256; ++i) op.s[i] = ld_c(sop, i);
+    DmGeom g;
+    const unsigned q[2] = {q0, q1};
+    if (!dm_geometry(n, 2, q, ls_max_for(layout, log_tile), &g, dm_max_v_low())) return (int)cudaErrorInvalidValue;
+    return launch_engine_map(layout, log_tile, rho, n, g, op, as_stream(stream));
+}
+
 int orkan_cu_exp_diag(int layout, unsigned log_tile, void* data, unsigned n, const double* diag, double t,
                       void* stream) {
     if (!data || !diag || n > 62) return (int)cudaErrorInvalidValue;

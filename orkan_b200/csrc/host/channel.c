@@ -5,6 +5,7 @@
 #include "internal.h"
 
 #include "channel.h"
+#include "orkan_dev.h"
 
 #define CHANNEL_VALIDATE(cond, msg) ORKAN_VALIDATE("channel", cond, msg)
 
@@ -60,4 +61,20 @@ void channel_1q(state_t *state, const superop_t *sop, const qubit_t target) {
         default:
             CHANNEL_VALIDATE(0, "channel_1q: unknown state type");
     }
+}
+
+/* 2-qubit channel (extension, include/orkan_dev.h): the reference's channel_1q accepts
+ * 1-local superoperators only (channel.c:67-85), although kraus_to_superop builds them for
+ * any qubit count.  Local index 2 * bit(q0) + bit(q1); vec index 4 * row + column. */
+void channel_2q(state_t *state, const superop_t *sop, const qubit_t q0, const qubit_t q1) {
+    CHANNEL_VALIDATE(state && state->data, "channel_2q: null state or data pointer");
+    CHANNEL_VALIDATE(q0 < state->qubits && q1 < state->qubits, "channel_2q: qubit out of range");
+    CHANNEL_VALIDATE(q0 != q1, "channel_2q: q0 and q1 must differ");
+    CHANNEL_VALIDATE(sop && sop->data, "channel_2q: null superoperator or data pointer");
+    CHANNEL_VALIDATE(sop->n_qubits == 2, "channel_2q: superoperator is not 2-local");
+    CHANNEL_VALIDATE(state->type == MIXED_PACKED || state->type == MIXED_TILED,
+                     "channel_2q: not available for pure states");
+    orkan_check_cu("channel", "channel_2q",
+                   orkan_cu_dm_superop2((int)state->type, LOG_TILE_DIM, state->data, state->qubits, q0, q1,
+                                        (const double *)sop->data, orkan_stream()));
 }

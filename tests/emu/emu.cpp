@@ -277,6 +277,16 @@ int emu_dm_superop1(int layout, unsigned log_tile, double* rho, uint64_t len, un
     return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
 }
 
+int emu_dm_superop2(int layout, unsigned log_tile, double* rho, uint64_t len, unsigned n, unsigned q0, unsigned q1,
+                    const double* sop, uint32_t* reads, uint32_t* writes, uint64_t* oob) {
+    OpSuper2 op;
+    for (unsigned i = 0; i < 256; ++i) op.s[i] = ldc(sop, i);
+    DmGeom g;
+    const unsigned q[2] = {q0, q1};
+    if (!dm_geometry(n, 2, q, ls_max_for(layout, log_tile), &g, emu_max_v())) return -1;
+    return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
+}
+
 int emu_dm_phase(int layout, unsigned log_tile, double* rho, uint64_t len, unsigned n, unsigned k,
                  const unsigned* qubits, const double* phase, uint32_t* reads, uint32_t* writes, uint64_t* oob) {
     EmuMem mem{reinterpret_cast<double2*>(rho), len, reads, writes, oob};

@@ -99,6 +99,13 @@ def dm_superop1(layout, lt, data, n, target, sop):
                                              _ptr(r), _ptr(w), C.byref(b)))
 
 
+def dm_superop2(layout, lt, data, n, q0, q1, sop):
+    s = _arr(np.asarray(sop).reshape(-1), np.complex128)
+    f = lib().emu_dm_superop2
+    return _run(f, data, lambda o, r, w, b: (LAYOUT[layout], lt, _ptr(o), C.c_uint64(o.size), n, q0, q1, _ptr(s),
+                                             _ptr(r), _ptr(w), C.byref(b)))
+
+
 def dm_exp_diag(layout, lt, data, n, diag, t):
     dg = _arr(diag, np.float64)
     f = lib().emu_dm_exp_diag

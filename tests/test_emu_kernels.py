@@ -145,6 +145,43 @@ def test_dm_superop_emulated(kind, lt, n):
             check_engine_counts(kind, n, lt, res)
 
 
+def random_cptp_2q(rng, terms=4):
+    """Kraus operators of a random 2-qubit channel: blocks of a 4*terms x 4 isometry."""
+    a = rng.normal(size=(4 * terms, 4)) + 1j * rng.normal(size=(4 * terms, 4))
+    q, _ = np.linalg.qr(a)
+    return [q[4 * k:4 * k + 4, :] for k in range(terms)]
+
+
+def test_superop2_oracle_is_the_kraus_sum():
+    """The 2-qubit superoperator restatement against sum_a K_a rho K_a^dagger with the
+    pinned Kronecker embedding (local index 2 bit(q0) + bit(q1), q0 the high bit)."""
+    rng = np.random.default_rng(5)
+    n = 4
+    rho = rand_rho(n, 9)
+    kr = random_cptp_2q(rng)
+    sop = R.kraus_to_superop(kr)
+    for q0, q1 in itertools.permutations(range(n), 2):
+        want = sum(R.apply_left(R.apply_left(rho, k, [q0, q1], n).conj().T, k, [q0, q1], n).conj().T for k in kr)
+        assert np.abs(R.apply_superop2(rho, sop, q0, q1) - want).max() < 1e-13
+
+
+@pytest.mark.parametrize("kind,lt", LAYOUTS)
+@pytest.mark.parametrize("n", [2, 3, 5, 7])
+def test_dm_superop2_emulated(kind, lt, n):
+    rng = np.random.default_rng(40 + n)
+    rho = rand_rho(n, 400 + n)
+    st = R.to_storage(kind, rho, lt)
+    sop = R.kraus_to_superop(random_cptp_2q(rng))
+    pairs = list(itertools.permutations(range(n), 2))
+    if len(pairs) > 24:
+        pairs = [pairs[i] for i in rng.choice(len(pairs), 24, replace=False)]
+    for q0, q1 in pairs:
+        res = kemu.dm_superop2(kind, lt, st, n, q0, q1, sop)
+        exp = R.to_storage(kind, R.apply_superop2(rho, sop, q0, q1), lt)
+        assert np.abs(res.out - exp).max() <= TOL, (q0, q1)
+        check_engine_counts(kind, n, lt, res)
+
+
 @pytest.mark.parametrize("kind,lt", LAYOUTS)
 @pytest.mark.parametrize("n", [1, 2, 4, 7])
 def test_dm_exp_diag_emulated(kind, lt, n):

@@ -127,6 +127,31 @@ def test_channels(request, lt, kind):
 
 
 @pytest.mark.parametrize("lt", [3, 5])
+@pytest.mark.parametrize("kind", ["packed", "tiled"])
+def test_channel_2q(request, lt, kind):
+    """2-qubit channels (channel_2q, an extension: the reference's channel_1q is 1-local):
+    kraus_to_superop of a random 4-term 2-qubit CPTP map, applied on ordered qubit pairs,
+    against the oracle's restatement (itself checked against the Kraus sum)."""
+    ork = lib_for(request, lt)
+    rng = np.random.default_rng(8)
+    for n in (2, 3, 5, 7):
+        rho = rand_rho(n, 80 + n)
+        st = ork.state(kind, n, R.to_storage(kind, rho, lt))
+        iso, _ = np.linalg.qr(rng.standard_normal((16, 4)) + 1j * rng.standard_normal((16, 4)))
+        kr = [iso[4 * i:4 * i + 4, :] for i in range(4)]
+        sop = ork.superop(kr)
+        assert np.abs(sop - R.kraus_to_superop(kr)).max() <= TOL
+        pairs = list(itertools.permutations(range(n), 2))
+        if len(pairs) > 20:
+            pairs = [pairs[i] for i in rng.choice(len(pairs), 20, replace=False)]
+        for q0, q1 in pairs:
+            ork.channel_2q(st, sop, int(q0), int(q1))
+            rho = R.apply_superop2(rho, sop, q0, q1)
+        assert np.abs(ork.storage(st) - R.to_storage(kind, rho, lt)).max() <= TOL
+        ork.free(st)
+
+
+@pytest.mark.parametrize("lt", [3, 5])
 @pytest.mark.parametrize("kind", ["pure", "packed", "tiled"])
 def test_mean_exp_diag(request, lt, kind):
     ork = lib_for(request, lt)
