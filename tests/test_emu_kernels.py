@@ -82,7 +82,7 @@ def gate_cases(n, max_ccx=60, seed=0):
 
 
 @pytest.mark.parametrize("kind,lt", LAYOUTS)
-@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 6, 7, 8])
 def test_dm_gates_emulated(kind, lt, n):
     rho = rand_rho(n, 100 + n)
     st = R.to_storage(kind, rho, lt)
