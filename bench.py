@@ -49,6 +49,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--batch-instances", type=int, default=4096, help="instances of the batched QAOA leg (0: skip)")
+    ap.add_argument("--batch-check", type=int, default=-1,
+                    help="batch instances checked against the per-call path (-1: every instance)")
     ap.add_argument("--surrogate-pairs", type=int, default=8192,
                     help="training pairs of the surrogate leg (65536: the full configuration; 0: skip)")
     ap.add_argument("--channel-qubits", type=int, default=13,
@@ -175,13 +177,19 @@ def measured_peak():
 
 
 def profiled_traffic():
-    """dram bytes per launch of each kernel class from the committed ncu summary."""
+    """ncu DRAM traffic of each kernel class from the committed summary: {class: (dram bytes
+    of the captured launch, algorithmic bytes of that launch)}."""
     path = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
     try:
         with open(path) as f:
-            return json.load(f)
+            raw = json.load(f)
     except Exception:
         return {}
+    out = {}
+    for c, v in raw.items():
+        if isinstance(v, dict) and v.get("dram_bytes") and v.get("algorithmic_bytes"):
+            out[c] = (float(v["dram_bytes"]), float(v["algorithmic_bytes"]))
+    return out
 
 
 # ---------------------------------------------------------------------------------------
@@ -220,24 +228,42 @@ def time_reference_sample(lib, states, plan, stride, offset):
     return nbytes, secs
 
 
+# The reference's CPU sample: every SAMPLE_STRIDE-th gate of the sweep (76 of its 1056 gate
+# applications, about 8 s on 16 host cores), the same gates in the cpu_baseline of the GPU
+# arm and in every step of the reference arm.
+SAMPLE_STRIDE = 14
+
+
+def sweep_config(npure: int, nmix: int, plan) -> dict:
+    """The workload description shared by both arms."""
+    return {"workload": f"single-gate throughput sweep: {npure} q PURE statevector + {nmix} q tiled and packed "
+                        f"density matrices, {len(plan)} gate applications per step",
+            "pure_qubits": npure, "mixed_qubits": nmix, "gates_per_step": len(plan),
+            "algorithmic_bytes_per_step": sum(e[5] for e in plan),
+            "l2": "inputs larger than L2 (16 GiB and 2.15 GB states vs 126 MB L2); no flush"}
+
+
+def sample_text(plan, cores, secs=None) -> str:
+    nsel = len(plan[::SAMPLE_STRIDE])
+    t = f", {secs:.1f} s" if secs is not None else ""
+    npure = next(e[1] for e in plan if e[0] == "pure")
+    nmix = next(e[1] for e in plan if e[0] != "pure")
+    return (f"every {SAMPLE_STRIDE}th gate of the sweep ({nsel} of {len(plan)} gate applications{t}) on the same "
+            f"states ({npure} q PURE, {nmix} q tiled, {nmix} q packed), OpenMP threads = {cores}")
+
+
 def cpu_baseline(plan, npure, nmix, budget_s):
     cores = host_cores()
     lib = reference_lib(cores)
     if lib is None:
         return None
     states = reference_states(lib, npure, nmix)
-    # warm the pages, then time a strided sample sized to the budget
-    first = [(i, e) for i, e in enumerate(plan)]
-    t0 = time.perf_counter()
-    lib.gate(states["pure"], "h", (0,))
-    est = max(time.perf_counter() - t0, 1e-3)
-    stride = max(1, int(math.ceil(len(plan) * est / budget_s)))
-    nbytes, secs = time_reference_sample(lib, states, plan, stride, 0)
+    lib.gate(states["pure"], "h", (0,))                    # warm the pages
+    nbytes, secs = time_reference_sample(lib, states, plan, SAMPLE_STRIDE, 0)
     for s in states.values():
         lib.free(s)
     return {"value": nbytes / secs / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"every {stride}th gate of the sweep ({len(first[::stride])} gates, {secs:.1f} s) on the same "
-                      f"{npure} q PURE / {nmix} q tiled / {nmix} q packed states, OpenMP threads = {cores}"}
+            "sample": sample_text(plan, cores, secs)}
 
 
 def run_reference(args):
@@ -247,38 +273,29 @@ def run_reference(args):
     plan = build_plan(args.pure_qubits, args.mixed_qubits)
     cores = host_cores()
     lib = reference_lib(cores)
-    config = {"workload": f"single-gate throughput sweep: {args.pure_qubits} q PURE, {args.mixed_qubits} q tiled "
-                          f"and packed density matrices, {len(plan)} gate applications per full sweep",
-              "pure_qubits": args.pure_qubits, "mixed_qubits": args.mixed_qubits, "sample": "strided"}
+    config = dict(sweep_config(args.pure_qubits, args.mixed_qubits, plan), parallelism="replicas x1")
     if lib is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/liborkan_ref_t5.so not built"}))
         return 0
     states = reference_states(lib, args.pure_qubits, args.mixed_qubits)
-    t0 = time.perf_counter()
-    lib.gate(states["pure"], "h", (0,))
-    est = max(time.perf_counter() - t0, 1e-3)
-    stride = max(1, int(math.ceil(len(plan) * est / 8.0)))     # about 8 s of gate work per step
     for w in range(args.warmup):
-        time_reference_sample(lib, states, plan, stride, w)
+        time_reference_sample(lib, states, plan, SAMPLE_STRIDE, 0)
     tot_b, tot_s = 0, 0.0
     for k in range(args.steps):
-        b, s = time_reference_sample(lib, states, plan, stride, args.warmup + k)
+        b, s = time_reference_sample(lib, states, plan, SAMPLE_STRIDE, 0)
         tot_b += b
         tot_s += s
     value = tot_b / tot_s / 1e9
-    sample = (f"every {stride}th gate of the sweep per step ({args.steps} steps, {tot_s:.1f} s of gate time), "
-              f"OpenMP threads = {cores}")
+    sample = sample_text(plan, cores) + f" per step ({args.steps} steps, {tot_s:.1f} s of gate time)"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded Gaussian states, uniform angles)", "config": config,
+            "data": "synthetic (seeded Gaussian states, Dirichlet mixtures, uniform angles)", "config": config,
+            "sample": sample,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
-
-
-
 
 
 # ---------------------------------------------------------------------------------------
@@ -481,10 +498,11 @@ def batched_leg(args, ork, clocks_cls, local, dist=None, rank=0, world=1):
                if bt is not None else {})
     line = None
     if rank == 0:
-        # every instance of a 64-instance sample of this rank's share against the per-call
-        # plain path of this library (the gathered vector holds the batch's means)
-        rng = np.random.default_rng(5)
-        pick = rng.choice(len(sh.idx), min(64, len(sh.idx)), replace=False)
+        # instances of this rank's share against the per-call plain path of this library
+        # (every instance by default; the gathered vector holds the batch's means)
+        nchk = len(sh.idx) if args.batch_check < 0 else min(args.batch_check, len(sh.idx))
+        pick = (np.arange(len(sh.idx)) if nchk == len(sh.idx)
+                else np.random.default_rng(5).choice(len(sh.idx), nchk, replace=False))
         errs, t_plain, amps_plain = [], 0.0, 0.0
         for j in pick:
             i = int(sh.idx[j])
@@ -513,7 +531,9 @@ def batched_leg(args, ork, clocks_cls, local, dist=None, rank=0, world=1):
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak * world, "peak_source": peak_kind,
                              "unit": "GB/s", "frac": achieved / (peak * world),
                              "algorithmic_bytes_per_amplitude": per_amp},
-                "checked_vs_plain": {"instances": len(errs), "max_abs_err": max(errs), "tolerance": 1e-12},
+                "checked_vs_plain": {"instances": len(errs), "of": len(sh.idx), "max_abs_err": max(errs),
+                                     "tolerance": 1e-12, "passed": bool(max(errs) <= 1e-12),
+                                     "seconds": t_plain},
                 "plain_per_call_gpu_evals_per_s": plain_evals,
                 "speedup_vs_plain_per_call": (count / (ms * 1e-3)) / plain_evals,
                 "cpu_baseline": cpu, "clocks": clocks}
@@ -738,12 +758,19 @@ def run_gpu(args):
     avg_ms = per_class_ms[dom] / launches_dom
     avg_bytes = per_class_bytes[dom] / launches_dom
     achieved = avg_bytes / (avg_ms * 1e-3) / 1e9
-    traffic = profiled_traffic().get(dom)
+    prof = profiled_traffic()
+    traffic = prof[dom][0] / prof[dom][1] * avg_bytes if dom in prof else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
                 "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "algorithmic_bytes_per_launch": avg_bytes, "avg_launch_ms": avg_ms, "launches": launches_dom}
     classes = {c: {"launches": per_class_n[c], "ms": per_class_ms[c], "share": per_class_ms[c] / sum(per_class_ms.values()),
                    "GB/s": per_class_bytes[c] / (per_class_ms[c] * 1e-3) / 1e9} for c in sorted(per_class_ms)}
+    # compact per-class table beside the dominant kernel: achieved GB/s, fraction of the
+    # measured peak, and ncu DRAM traffic / algorithmic bytes where a capture is committed
+    roofline["classes"] = {
+        c: {"GB/s": round(v["GB/s"], 1), "frac": round(v["GB/s"] / peak, 3), "share": round(v["share"], 3),
+            "traffic_ratio": (round(prof[c][0] / prof[c][1], 3) if c in prof else None)}
+        for c, v in classes.items()}
     by_gate = {}
     for k in range(args.steps):
         prev = start if k == 0 else ev[k - 1][-1]
@@ -778,13 +805,8 @@ def run_gpu(args):
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded Gaussian states, Dirichlet mixtures, uniform angles)",
-                "config": {"workload": f"single-gate throughput sweep: {args.pure_qubits} q PURE statevector + "
-                                       f"{args.mixed_qubits} q tiled and packed density matrices, "
-                                       f"{len(plan)} gate applications per step",
-                           "pure_qubits": args.pure_qubits, "mixed_qubits": args.mixed_qubits,
-                           "gates_per_step": len(plan), "algorithmic_bytes_per_step": step_bytes,
-                           "l2": "inputs larger than L2 (16 GiB and 2.15 GB states vs 126 MB L2); no flush",
-                           "parallelism": f"replicas x{world}"},
+                "config": dict(sweep_config(args.pure_qubits, args.mixed_qubits, plan),
+                               parallelism=f"replicas x{world}"),
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": launches, "kernel_classes": classes, "by_gate": gates,
                 "observables": observables, "channels": channels, "batched": batched, "surrogate": surrogate, "surrogate_noisy": noisy}

@@ -123,6 +123,16 @@ int orkan_cu_exp_diag_noalloc(int layout, unsigned log_tile, void *data, unsigne
  * waiting forever).  Reads device memory, so it synchronises with the device. */
 unsigned orkan_cu_engine_status(void);
 
+/* Reset the engine's error word to 0 on the current device (synchronises). */
+int orkan_cu_engine_status_clear(void);
+
+/* Test hook of the failure path: polls > 0 limits each of the engine's waits for staged
+ * data to that many polls (0 restores the default of 2^24); drop_loads != 0 (with polls > 0)
+ * arms each item's completion barrier but issues none of its copies, so the wait runs out
+ * with nothing in flight and the kernel returns early with bit 0 of the error word set.
+ * The state's contents are unspecified after such a launch.  Not for production use. */
+void orkan_cu_engine_test_wait(unsigned long long polls, int drop_loads);
+
 /* Number of kernels this library has launched in this process (all devices). */
 unsigned long long orkan_cu_launch_count(void);
 

@@ -53,6 +53,9 @@ struct DmGeom {
     unsigned long long fixrows;  // the same as a mask over virtual indices (dm_fixed_rows)
     unsigned long long hcmask;   // controlled flips: control qubits above the sub-tile that are
                                  // not pairing bits (one value per item's rows or columns)
+    unsigned long long wait_limit = 1ull << 24;   // polls of a bounded wait for staged data
+    unsigned drop_loads = 0;     // test hook: arm the barrier but issue no copy, so the wait
+                                 // for the item's data runs out (nothing is in flight)
     ORKAN_HD unsigned S() const { return 1u << ls; }
     ORKAN_HD unsigned V() const { return 1u << (ls + h); }
     ORKAN_HD unsigned P() const { return V() + 1; }    // smem row pitch (padded)
@@ -815,11 +818,10 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 
 // Error word of the engine: bit 0 set when a wait for staged data ran past its limit.
 __device__ unsigned int g_dm_engine_error;
-constexpr unsigned long long kDmWaitLimit = 1ull << 24;
 
 // Bounded wait for the copies of a stage (false: limit reached, error recorded).
-__device__ __forceinline__ bool dm_wait_stage(unsigned long long* bar, unsigned parity) {
-    for (unsigned long long i = 0; i < kDmWaitLimit; ++i)
+__device__ __forceinline__ bool dm_wait_stage(unsigned long long* bar, unsigned parity, unsigned long long limit) {
+    for (unsigned long long i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     atomicOr(&g_dm_engine_error, 1u);
     return false;
@@ -865,11 +867,11 @@ __global__ void __launch_bounds__(kDmBlock, DmMinBlocks<Op>::value) k_dm_engine(
         // every thread issues its share of the bulk loads (a warp issues them one after
         // another, so one issuing warp would cap the block's copy rate)
         fence_proxy_async();
-        dm_bulk_loads(mem, map, g, pd, vb, bar, tid, nthr);
+        if (!g.drop_loads) dm_bulk_loads(mem, map, g, pd, vb, bar, tid, nthr);
         const unsigned long long fix0 = dm_pass_mask<Map>(pd, npos, 0);
         const unsigned long long fix1 = dm_pass_mask<Map>(pd, npos, 1);
         const unsigned long long mirr = dm_pass_mask<Map>(pd, npos, 2);
-        ok = __syncthreads_and(dm_wait_stage(bar, parity) ? 1 : 0) != 0;
+        ok = __syncthreads_and(dm_wait_stage(bar, parity, g.wait_limit) ? 1 : 0) != 0;
         parity ^= 1u;
         if (!ok) break;
         if (fix0) {
@@ -892,7 +894,7 @@ __global__ void __launch_bounds__(kDmBlock, DmMinBlocks<Op>::value) k_dm_engine(
     }
     if (!ok) {
         // give copies still in flight a bounded chance to land before the block exits
-        for (unsigned long long i = 0; i < kDmWaitLimit && !mbar_try_wait(bar, parity); ++i) {
+        for (unsigned long long i = 0; i < g.wait_limit && !mbar_try_wait(bar, parity); ++i) {
         }
     }
     bulk_wait_all();

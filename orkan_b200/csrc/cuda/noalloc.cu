@@ -16,9 +16,11 @@
 // on different streams) race on the table.
 #include "common.cuh"
 #include "dm_phase.cuh"
+#include "launch.cuh"
 
 #include "../../../include/orkan_cu.h"
 
+#include <mutex>
 #include <stdio.h>
 
 using namespace orkan;
@@ -32,7 +34,9 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double2 g_noalloc_table[kNoAllocMaxDim];
 
 // Device address of g_noalloc_table, resolved once per device by the first call made on
-// that device (host code cannot use the symbol itself as a device pointer).
+// that device (host code cannot use the symbol itself as a device pointer).  The mutex
+// serialises first calls made from several host threads at once.
+std::mutex g_table_mu;
 double2* g_table_addr[kMaxDevices] = {};
 
 struct TabMem {
@@ -53,6 +57,7 @@ int table_address(double2** out) {
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return (int)e;
     if (dev < 0 || dev >= kMaxDevices) return (int)cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_table_mu);
     if (!g_table_addr[dev]) {
         void* ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, g_noalloc_table);
@@ -81,17 +86,8 @@ extern "C" int orkan_cu_exp_diag_noalloc(int layout, unsigned log_tile, void* da
     int rc = table_address(&tab);
     if (rc) return rc;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const unsigned tgrid = (unsigned)((d + 255) / 256 < 1184 ? (d + 255) / 256 : 1184);
-    k_noalloc_table<<<tgrid, 256, 0, st>>>(diag, d, t, tab);
-    rc = (int)cudaGetLastError();
+    k_noalloc_table<<<grid_for(256, d, (unsigned)sm_count() * 8u), 256, 0, st>>>(diag, d, t, tab);
+    rc = finish_launch();
     if (rc) return rc;
-    const PhaseGeom g = phase_geometry(n, layout == 2 ? log_tile : 5u);
-    const unsigned grid = (unsigned)(g.items < 148u * 32u ? g.items : 148u * 32u);
-    TableFactor<TabMem> fac{TabMem{tab}};
-    DevMem mem{static_cast<double2*>(data)};
-    if (layout == 1)
-        k_dm_phase<PackedMap, TableFactor<TabMem>><<<grid, kPhaseThreads, 0, st>>>(mem, PackedMap{d}, g, fac);
-    else
-        k_dm_phase<TiledMap, TableFactor<TabMem>><<<grid, kPhaseThreads, 0, st>>>(mem, TiledMap{d, log_tile}, g, fac);
-    return (int)cudaGetLastError();
+    return launch_phase(layout, log_tile, data, n, TableFactor<TabMem>{TabMem{tab}}, st);
 }

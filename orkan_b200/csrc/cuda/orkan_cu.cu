@@ -4,6 +4,7 @@
 #include "common.cuh"
 #include "dm_engine.cuh"
 #include "dm_phase.cuh"
+#include "launch.cuh"
 #include "pure.cuh"
 #include "reduce.cuh"
 #include "scratch.cuh"
@@ -17,34 +18,37 @@
 using namespace orkan;
 
 namespace {
-
 std::atomic<unsigned long long> g_launches{0};
+std::atomic<int> g_sm_count[64];
+}  // namespace
 
-inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+namespace orkan {
 
 int sm_count() {
-    static int cached[64] = {0};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-    if (!cached[dev]) {
-        int v = 0;
+    int v = g_sm_count[dev].load(std::memory_order_relaxed);
+    if (v <= 0) {
         if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
-        cached[dev] = v;
+        g_sm_count[dev].store(v, std::memory_order_relaxed);
     }
-    return cached[dev];
+    return v;
 }
 
-inline unsigned grid_for(idx_t work_per_block_units, idx_t total_units, unsigned cap) {
-    idx_t g = (total_units + work_per_block_units - 1) / work_per_block_units;
-    if (g < 1) g = 1;
-    if (g > cap) g = cap;
-    return (unsigned)g;
-}
-
-inline int finish_launch() {
+int finish_launch() {
     g_launches.fetch_add(1, std::memory_order_relaxed);
     return (int)cudaGetLastError();
 }
+
+}  // namespace orkan
+
+namespace {
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Test hook of the engine's bounded waits (orkan_cu_engine_test_wait): 0 polls = the default.
+std::atomic<unsigned long long> g_engine_test_polls{0};
+std::atomic<unsigned> g_engine_test_drop{0};
 
 struct Complex8 { double2 v[8]; };
 
@@ -65,9 +69,12 @@ unsigned engine_grid(Kern kern, size_t smem, idx_t items) {
 }
 
 template <class Op>
-int launch_engine_map(int layout, unsigned log_tile, void* rho, unsigned n, const DmGeom& g, Op op,
-                      cudaStream_t st) {
+int launch_engine_map(int layout, unsigned log_tile, void* rho, unsigned n, DmGeom g, Op op, cudaStream_t st) {
     const size_t smem = dm_block_smem_bytes(g);
+    if (const unsigned long long polls = g_engine_test_polls.load(std::memory_order_relaxed)) {
+        g.wait_limit = polls;
+        g.drop_loads = g_engine_test_drop.load(std::memory_order_relaxed);
+    }
     dm_orient(op, layout == 1);               // the packed layout stages rho^T
     DevMemBulk mem{static_cast<double2*>(rho)};
     if (layout == 1) {
@@ -105,19 +112,6 @@ inline bool layout_ok(int layout, unsigned log_tile) {
 
 // sub-tile side limit: tiles for the tiled layout, 64 for packed
 inline unsigned ls_max_for(int layout, unsigned log_tile) { return layout == 2 ? log_tile : 6u; }
-
-template <class Factor>
-int launch_phase(int layout, unsigned log_tile, void* rho, unsigned n, const Factor& fac, cudaStream_t st) {
-    const PhaseGeom g = phase_geometry(n, layout == 2 ? log_tile : 5u);
-    const unsigned grid = grid_for(1, g.items, (unsigned)sm_count() * 32u);
-    DevMem mem{static_cast<double2*>(rho)};
-    if (layout == 1) {
-        k_dm_phase<PackedMap, Factor><<<grid, kPhaseThreads, 0, st>>>(mem, PackedMap{idx_t(1) << n}, g, fac);
-    } else {
-        k_dm_phase<TiledMap, Factor><<<grid, kPhaseThreads, 0, st>>>(mem, TiledMap{idx_t(1) << n, log_tile}, g, fac);
-    }
-    return finish_launch();
-}
 
 struct DevMemC2 {
     const double2* p;
@@ -314,31 +308,23 @@ int orkan_cu_exp_diag(int layout, unsigned log_tile, void* data, unsigned n, con
 int orkan_cu_mean(int layout, unsigned log_tile, const void* data, unsigned n, const double* obs, double* result,
                   void* stream) {
     if (!data || !obs || !result || n > 62) return (int)cudaErrorInvalidValue;
+    if (layout != 0 && !layout_ok(layout, log_tile)) return (int)cudaErrorInvalidValue;
     cudaStream_t st = as_stream(stream);
     const idx_t d = idx_t(1) << n;
-    const unsigned np = grid_for(kRedThreads * 4, d, kRedBlocks);
+    // PURE: 4 amplitudes per thread per block at least; DM: one diagonal element per thread
+    const unsigned np = grid_for(layout == 0 ? kRedThreads * 4 : kRedThreads, d, kRedBlocks);
     double* part = static_cast<double*>(scratch_get((np + 1) * sizeof(double)));
     if (!part) return (int)cudaErrorMemoryAllocation;
     double* out = part + np;
-    if (layout == 0) {
-        k_mean_pure_partial<<<np, kRedThreads, 0, st>>>(static_cast<const double2*>(data), obs, d, part);
-        int rc = finish_launch();
-        if (rc) return rc;
-        k_fold_partials<<<1, kRedThreads, 0, st>>>(part, np, 1, out);
-        rc = finish_launch();
-        if (rc) return rc;
-    } else if (layout == 1) {
-        k_mean_dm<PackedMap><<<1, kDiagThreads, 0, st>>>(static_cast<const double2*>(data), PackedMap{d}, obs, out);
-        const int rc = finish_launch();
-        if (rc) return rc;
-    } else if (layout_ok(layout, log_tile)) {
-        k_mean_dm<TiledMap><<<1, kDiagThreads, 0, st>>>(static_cast<const double2*>(data), TiledMap{d, log_tile}, obs,
-                                                        out);
-        const int rc = finish_launch();
-        if (rc) return rc;
-    } else {
-        return (int)cudaErrorInvalidValue;
-    }
+    const double2* rho = static_cast<const double2*>(data);
+    if (layout == 0)
+        k_mean_pure<<<np, kRedThreads, 0, st>>>(rho, obs, d, part, out);
+    else if (layout == 1)
+        k_mean_dm<PackedMap><<<np, kRedThreads, 0, st>>>(rho, PackedMap{d}, obs, part, out);
+    else
+        k_mean_dm<TiledMap><<<np, kRedThreads, 0, st>>>(rho, TiledMap{d, log_tile}, obs, part, out);
+    const int rc = finish_launch();
+    if (rc) return rc;
     cudaError_t e = cudaMemcpyAsync(result, out, sizeof(double), cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return (int)e;
     return (int)cudaStreamSynchronize(st);
@@ -353,12 +339,9 @@ int orkan_cu_matel_diag(const void* bra, const void* ket, unsigned n, const doub
     double* part = static_cast<double*>(scratch_get((2 * np + 2) * sizeof(double)));
     if (!part) return (int)cudaErrorMemoryAllocation;
     double* out = part + 2 * np;
-    k_matel_pure_partial<<<np, kRedThreads, 0, st>>>(static_cast<const double2*>(bra),
-                                                     static_cast<const double2*>(ket), obs, d, part);
-    int rc = finish_launch();
-    if (rc) return rc;
-    k_fold_partials<<<1, kRedThreads, 0, st>>>(part, np, 2, out);
-    rc = finish_launch();
+    k_matel_pure<<<np, kRedThreads, 0, st>>>(static_cast<const double2*>(bra), static_cast<const double2*>(ket), obs,
+                                             d, part, out);
+    const int rc = finish_launch();
     if (rc) return rc;
     cudaError_t e = cudaMemcpyAsync(result, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return (int)e;
@@ -372,6 +355,16 @@ unsigned orkan_cu_engine_status(void) {
     unsigned v = 0;
     if (cudaMemcpyFromSymbol(&v, g_dm_engine_error, sizeof(v)) != cudaSuccess) return 0xffffffffu;
     return v;
+}
+
+int orkan_cu_engine_status_clear(void) {
+    const unsigned zero = 0;
+    return (int)cudaMemcpyToSymbol(g_dm_engine_error, &zero, sizeof(zero));
+}
+
+void orkan_cu_engine_test_wait(unsigned long long polls, int drop_loads) {
+    g_engine_test_drop.store(polls && drop_loads ? 1u : 0u, std::memory_order_relaxed);
+    g_engine_test_polls.store(polls, std::memory_order_relaxed);
 }
 
 }  // extern "C"

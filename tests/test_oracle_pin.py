@@ -201,3 +201,33 @@ def test_known_answers_restatement():
     ref = np.zeros((4, 4))
     ref[0, 3] = ref[1, 2] = ref[2, 1] = ref[3, 0] = 1
     assert np.abs(s - ref).max() <= TOL
+
+
+@pytest.mark.parametrize("lt", [3, 5])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 6, 7])
+def test_matrix_gates_match_reference(request, lt, n):
+    """single_from_mat / two_from_mat (reference src/gate/tiled/gate_tiled_1q.c:3-184,
+    gate_tiled_2q.c:3-60) on tiled states: mat is column-major, the 4 x 4 local index is
+    bit(lo) + 2 bit(hi) whatever the argument order, and rho -> mat rho mat^dagger.  The
+    oracle's conjugate_by with qubits (hi, lo) (first listed qubit = most significant local
+    bit) must agree on every target and every ordered pair."""
+    ref = request.getfixturevalue(f"ref{lt}")
+    rng = np.random.default_rng(77 * lt + n)
+    for q in range(n):
+        rho = rand_rho(n, int(rng.integers(1 << 30)))
+        u, _ = np.linalg.qr(rng.standard_normal((2, 2)) + 1j * rng.standard_normal((2, 2)))
+        st = ref.state("tiled", n, R.to_storage("tiled", rho, lt))
+        ref.single_from_mat(st, q, u.reshape(-1, order="F"))
+        out = ref.storage(st)
+        ref.free(st)
+        exp = R.to_storage("tiled", R.conjugate_by(rho, u, [q], n), lt)
+        assert np.abs(out - exp).max() <= TOL, q
+    for q1, q2 in itertools.permutations(range(n), 2):
+        rho = rand_rho(n, int(rng.integers(1 << 30)))
+        u, _ = np.linalg.qr(rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4)))
+        st = ref.state("tiled", n, R.to_storage("tiled", rho, lt))
+        ref.two_from_mat(st, q1, q2, u.reshape(-1, order="F"))
+        out = ref.storage(st)
+        ref.free(st)
+        exp = R.to_storage("tiled", R.conjugate_by(rho, u, [max(q1, q2), min(q1, q2)], n), lt)
+        assert np.abs(out - exp).max() <= TOL, (q1, q2)
