@@ -53,6 +53,8 @@ def parse_args():
                     help="batch instances checked against the per-call path (-1: every instance)")
     ap.add_argument("--surrogate-pairs", type=int, default=8192,
                     help="training pairs of the surrogate leg (65536: the full configuration; 0: skip)")
+    ap.add_argument("--circuit-gates", type=int, default=200,
+                    help="gates of the fused-circuit leg on the PURE statevector (0: skip)")
     ap.add_argument("--channel-qubits", type=int, default=13,
                     help="density-matrix qubits of the Kraus-channel leg (0: skip)")
     ap.add_argument("--noisy-pairs", type=int, default=0,
@@ -339,6 +341,64 @@ def observables_leg(args, ork, states, obs_dev):
             v["frac"] = v["GB/s"] / peak
         out[kind] = res
     return out
+
+# ---------------------------------------------------------------------------------------
+# fused-circuit leg: a random circuit on the PURE statevector with gate fusion on and off
+# ---------------------------------------------------------------------------------------
+def circuit_leg(args, ork, clocks_cls, local):
+    """A random circuit of the parity configuration's kind (gates uniform over the 18 calls,
+    distinct qubits uniform, angles U[0, 2 pi)) on the 30-qubit statevector, timed through
+    the public gate calls with statevector gate fusion on (runs of gates per pass) and off
+    (one pass per gate).  Reports gates/s, the passes over the state each way, and the
+    algorithmic bytes per gate (one dense pass = 2 x 16 GiB) over the time of the run."""
+    import torch
+    from orkan_b200 import traffic as T
+    from orkan_b200 import workloads as W
+    n, ng = args.pure_qubits, args.circuit_gates
+    gates = W.random_circuit(n, ng, seed=2024)
+    alg = sum(T.gate_bytes("pure", n, g, qs, 5) for g, qs, _ in gates)
+    st = ork.state("pure", n)
+    W.fill_state_on_device(ork, st, "pure", n, seed=11, log_tile=5)
+    peak, peak_kind = measured_peak()
+    out = {"metric": "circuit gates/s", "config": {"workload": f"{ng}-gate random circuit (gates uniform over the "
+                                                               f"18 calls, distinct qubits uniform, angles U[0, 2 pi)) "
+                                                               f"on the {n} q PURE statevector",
+                                                   "gates": ng, "algorithmic_bytes": alg}}
+    for label, cap in (("fused", 48), ("unfused", 0)):
+        ork.set_gate_fusion(cap)
+        for _ in range(2):                                   # warm-up
+            for g, qs, th in gates:
+                ork.gate(st, g, qs, th)
+        ork.flush()
+        torch.cuda.synchronize()
+        steps = max(1, args.steps)
+        clk = clocks_cls(local)
+        clk.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ork.launches()
+        e0.record()
+        for _ in range(steps):
+            for g, qs, th in gates:
+                ork.gate(st, g, qs, th)
+            ork.flush()
+        e1.record()
+        torch.cuda.synchronize()
+        clocks = clk.stop()
+        launches = (ork.launches() - l0) / steps
+        ms = e0.elapsed_time(e1) / steps
+        state_bytes = 16 * (1 << n)
+        out[label] = {"ms": ms, "gates_per_s": ng / (ms * 1e-3), "launches": launches,
+                      "gates_per_launch": ng / launches,
+                      "algorithmic_GB/s": alg / (ms * 1e-3) / 1e9,
+                      "pass_GB/s": 2 * state_bytes * launches / (ms * 1e-3) / 1e9,
+                      "pass_frac_of_peak": 2 * state_bytes * launches / (ms * 1e-3) / 1e9 / peak,
+                      "clocks": clocks}
+    ork.set_gate_fusion(48)                                  # the library default
+    ork.free(st)
+    out["speedup"] = out["unfused"]["ms"] / out["fused"]["ms"]
+    out["peak_source"] = peak_kind
+    return out
+
 
 # ---------------------------------------------------------------------------------------
 # Kraus-channel leg: 13 q tiled and packed density matrices, four channel kinds per qubit
@@ -657,6 +717,9 @@ def run_gpu(args):
 
     ork = orkan_b200.load(5)
     ork.set_stream(torch.cuda.current_stream().cuda_stream)
+    # the sweep measures one-gate kernels: statevector gate fusion stays off for it (the
+    # circuit leg below measures fused runs)
+    ork.set_gate_fusion(0)
     plan = build_plan(args.pure_qubits, args.mixed_qubits)
     step_bytes = sum(e[5] for e in plan)
 
@@ -791,6 +854,8 @@ def run_gpu(args):
     observables = observables_leg(args, ork, states, obs_dev) if rank == 0 else None
     for st in states.values():
         ork.free(st)
+    ork.set_gate_fusion(48)                  # the library default from here on
+    circuit = circuit_leg(args, ork, ClockSampler, local) if rank == 0 and args.circuit_gates > 0 else None
     batched = surrogate = noisy = channels = None
     if rank == 0 and world == 1 and args.channel_qubits > 0:
         channels = channels_leg(args, ork, ClockSampler, local)
@@ -809,7 +874,7 @@ def run_gpu(args):
                                parallelism=f"replicas x{world}"),
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": launches, "kernel_classes": classes, "by_gate": gates,
-                "observables": observables, "channels": channels, "batched": batched, "surrogate": surrogate, "surrogate_noisy": noisy}
+                "observables": observables, "circuit": circuit, "channels": channels, "batched": batched, "surrogate": surrogate, "surrogate_noisy": noisy}
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

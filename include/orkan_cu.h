@@ -53,6 +53,30 @@ int orkan_cu_pure_gate2(void *psi, unsigned n, unsigned qa, unsigned qb, int op,
 /* Toffoli on a statevector.  Replaces ccx_pure (reference gate_pure.c:405-434). */
 int orkan_cu_pure_ccx(void *psi, unsigned n, unsigned c1, unsigned c2, unsigned t, void *stream);
 
+/* A run of statevector gates applied in one pass over the amplitudes.  Gate codes: the
+ * orkan_op1 codes (q[0] = target; c, s as for orkan_cu_pure_gate1) and the orkan_fop codes
+ * (CX/CY: q[0] control, q[1] target; CZ and SWAP: q[0], q[1]; CCX: q[0], q[1] controls,
+ * q[2] target).  The state is cut into chunks of 2^log_chunk amplitudes that differ in
+ * log_chunk "local" qubits: qubits 0-2 and every qubit a gate of the run mixes (the target
+ * of X/Y/H/Hy/Rx/Ry/CX/CY/CCX, both qubits of SWAP), filled up with the lowest free qubits.
+ * Each chunk is loaded once, every gate is applied to it in shared memory with the
+ * arithmetic of the one-gate kernels (bit-identical results), and it is stored once.
+ * No counterpart in the reference, which makes one pass per gate
+ * (src/gate/gate_pure.c:33-48 and :282-434).  1 <= ngates <= 48, log_chunk <= min(n, 12). */
+enum orkan_fop { ORKAN_FOP_CX = 16, ORKAN_FOP_CY, ORKAN_FOP_CZ, ORKAN_FOP_SWAP, ORKAN_FOP_CCX };
+typedef struct {
+    int op;
+    unsigned q[3];
+    double c, s;
+} orkan_fgate_t;
+
+int orkan_cu_pure_fused(void *psi, unsigned n, unsigned log_chunk, unsigned ngates, const orkan_fgate_t *gates,
+                        void *stream);
+
+/* The qubits gate g mixes (which a fused run must hold local), as a bit mask; all bits set
+ * for an invalid op code. */
+unsigned long long orkan_cu_fused_need(const orkan_fgate_t *g);
+
 /* rho -> U rho U^dagger for a dense k-qubit U (k = 1 or 2), u = 2^k x 2^k row-major
  * interleaved complex.  Replaces h/hy/rx/ry_{packed,tiled} and the generic
  * single_from_mat / two_from_mat (reference gate_packed_1q.c:126-677,

@@ -118,6 +118,10 @@ class Orkan:
         L.orkan_cu_launch_count.restype = C.c_ulonglong
         L.sample_matrix.argtypes = [P, vp, C.POINTER(SmChannel), C.c_uint, C.c_uint, C.c_size_t, vp]
         L.sample_matrix.restype = None
+        L.orkan_flush.restype = None
+        L.orkan_set_gate_fusion.argtypes = [C.c_uint]
+        L.orkan_set_gate_fusion.restype = None
+        L.orkan_get_gate_fusion.restype = C.c_uint
 
     # ---- states ------------------------------------------------------------------
     def state(self, kind: str, n: int, storage: np.ndarray | None = None) -> StateT:
@@ -250,6 +254,16 @@ class Orkan:
 
     def sync(self) -> None:
         self.lib.orkan_sync()
+
+    def flush(self) -> None:
+        """Launch queued statevector gates (see orkan_set_gate_fusion)."""
+        self.lib.orkan_flush()
+
+    def set_gate_fusion(self, max_gates: int) -> None:
+        self.lib.orkan_set_gate_fusion(int(max_gates))
+
+    def gate_fusion(self) -> int:
+        return int(self.lib.orkan_get_gate_fusion())
 
     def launches(self) -> int:
         return int(self.lib.orkan_launch_count())

@@ -29,7 +29,7 @@ CC_FLAGS = ["-std=gnu17", "-O2", "-fPIC", "-Wall", "-Wno-unused-function", "-I" 
             "-I" + os.path.join(CUDA_HOME, "include")]
 
 CU_SOURCES = ["orkan_cu.cu", "scratch.cu", "noalloc.cu", "qaoa.cu", "mlp.cu", "sample.cu"]
-C_SOURCES = ["runtime.c", "state.c", "gate.c", "channel.c", "meas.c", "circ.c", "sample.c"]
+C_SOURCES = ["runtime.c", "state.c", "gate.c", "fuse.c", "channel.c", "meas.c", "circ.c", "sample.c"]
 LIBS = {5: "liborkan_b200.so", 3: "liborkan_b200_t3.so"}
 
 

@@ -6,6 +6,7 @@
 #include "dm_phase.cuh"
 #include "launch.cuh"
 #include "pure.cuh"
+#include "pure_fused.cuh"
 #include "reduce.cuh"
 #include "scratch.cuh"
 
@@ -195,6 +196,28 @@ int orkan_cu_pure_ccx(void* psi, unsigned n, unsigned c1, unsigned c2q, unsigned
     k_pure_ccx<<<grid, kPureThreads, 0, as_stream(stream)>>>(DevMem{static_cast<double2*>(psi)}, no, c1, c2q, t);
     return finish_launch();
 }
+
+int orkan_cu_pure_fused(void* psi, unsigned n, unsigned log_chunk, unsigned ngates, const orkan_fgate_t* gates,
+                        void* stream) {
+    if (!psi || !gates) return (int)cudaErrorInvalidValue;
+    FusedPlan plan;
+    if (!fused_plan(n, log_chunk, ngates, gates, &plan)) return (int)cudaErrorInvalidValue;
+    const size_t smem = fused_smem_bytes(plan);
+    static std::atomic<bool> attr{false};
+    if (!attr.load(std::memory_order_relaxed)) {
+        cudaFuncSetAttribute(k_pure_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+        attr.store(true, std::memory_order_relaxed);
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pure_fused, kFuseThreads, smem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    const unsigned grid = grid_for(1, plan.nchunks(), (unsigned)(sm_count() * per_sm));
+    k_pure_fused<<<grid, kFuseThreads, smem, as_stream(stream)>>>(DevMem{static_cast<double2*>(psi)}, plan);
+    return finish_launch();
+}
+
+unsigned long long orkan_cu_fused_need(const orkan_fgate_t* g) { return g ? fused_need(*g) : ~0ull; }
 
 int orkan_cu_dm_unitary(int layout, unsigned log_tile, void* rho, unsigned n, unsigned k, const unsigned* qubits,
                         const double* u, void* stream) {

@@ -9,6 +9,7 @@
 #define CIRC_VALIDATE(cond, msg) ORKAN_VALIDATE("circ", cond, msg)
 
 static void exp_diag_layout(state_t *state, const double *diag, double t) {
+    orkan_flush();
     const size_t dim = (size_t)1 << state->qubits;
     const double *ddiag = orkan_device_doubles("circ", diag, dim);
     orkan_check_cu("circ", "exp_diag",

@@ -21,9 +21,14 @@
 
 static const double R2 = 0.70710678118654752440;   /* M_SQRT1_2 */
 
-/* ---- PURE backends ----------------------------------------------------------- */
+/* ---- PURE backends: gates join the statevector gate queue (fuse.c) --------------- */
 static void pure1(state_t *s, qubit_t q, int op, double c, double sn, const char *name) {
-    orkan_check_cu("gate", name, orkan_cu_pure_gate1(s->data, s->qubits, q, op, c, sn, orkan_stream()));
+    const orkan_fgate_t g = {op, {q, 0, 0}, c, sn};
+    orkan_pure_gate(s, &g, name);
+}
+static void pure2(state_t *s, qubit_t a, qubit_t b, int op, const char *name) {
+    const orkan_fgate_t g = {op, {a, b, 0}, 0.0, 0.0};
+    orkan_pure_gate(s, &g, name);
 }
 
 void x_pure(state_t *state, qubit_t target)   { pure1(state, target, ORKAN_OP_X, 0, 0, "x"); }
@@ -50,20 +55,13 @@ void p_pure(state_t *state, qubit_t target, double theta) {
     pure1(state, target, ORKAN_OP_P, cos(theta), sin(theta), "p");
 }
 
-void cx_pure(state_t *state, qubit_t control, qubit_t target) {
-    orkan_check_cu("gate", "cx", orkan_cu_pure_gate2(state->data, state->qubits, control, target, ORKAN_OP_CX, orkan_stream()));
-}
-void cy_pure(state_t *state, qubit_t control, qubit_t target) {
-    orkan_check_cu("gate", "cy", orkan_cu_pure_gate2(state->data, state->qubits, control, target, ORKAN_OP_CY, orkan_stream()));
-}
-void cz_pure(state_t *state, qubit_t control, qubit_t target) {
-    orkan_check_cu("gate", "cz", orkan_cu_pure_gate2(state->data, state->qubits, control, target, ORKAN_OP_CZ, orkan_stream()));
-}
-void swap_pure(state_t *state, qubit_t q1, qubit_t q2) {
-    orkan_check_cu("gate", "swap", orkan_cu_pure_gate2(state->data, state->qubits, q1, q2, ORKAN_OP_SWAP, orkan_stream()));
-}
+void cx_pure(state_t *state, qubit_t control, qubit_t target) { pure2(state, control, target, ORKAN_FOP_CX, "cx"); }
+void cy_pure(state_t *state, qubit_t control, qubit_t target) { pure2(state, control, target, ORKAN_FOP_CY, "cy"); }
+void cz_pure(state_t *state, qubit_t control, qubit_t target) { pure2(state, control, target, ORKAN_FOP_CZ, "cz"); }
+void swap_pure(state_t *state, qubit_t q1, qubit_t q2) { pure2(state, q1, q2, ORKAN_FOP_SWAP, "swap"); }
 void ccx_pure(state_t *state, qubit_t ctrl1, qubit_t ctrl2, qubit_t target) {
-    orkan_check_cu("gate", "ccx", orkan_cu_pure_ccx(state->data, state->qubits, ctrl1, ctrl2, target, orkan_stream()));
+    const orkan_fgate_t g = {ORKAN_FOP_CCX, {ctrl1, ctrl2, target}, 0.0, 0.0};
+    orkan_pure_gate(state, &g, "ccx");
 }
 
 /* ---- density-matrix backends (packed and tiled share the kernels) ---------------- */

@@ -32,6 +32,11 @@ void *orkan_stream(void);
  * host pointer is copied into the library's staging buffer. */
 const double *orkan_device_doubles(const char *module, const double *p, size_t n);
 
+/* Statevector gate queue (fuse.c): enqueue a gate on a PURE state (launched with the
+ * next flush, or at once when fusion is off); drop the queue of a state being freed. */
+void orkan_pure_gate(state_t *state, const orkan_fgate_t *g, const char *name);
+void orkan_fuse_drop(const void *data);
+
 /* Device allocation of len zeroed elements (NULL on failure or injected failure). */
 cplx_t *orkan_alloc_state(idx_t len);
 void orkan_free_device(void *p);

@@ -9,6 +9,7 @@
 #define MEAS_VALIDATE(cond, msg) ORKAN_VALIDATE("meas", cond, msg)
 
 static double mean_layout(const state_t *state, const double *obs) {
+    orkan_flush();
     const size_t dim = (size_t)1 << state->qubits;
     const double *dobs = orkan_device_doubles("meas", obs, dim);
     double r = 0.0;
@@ -22,6 +23,7 @@ double mean_packed(const state_t *state, const double *obs) { return mean_layout
 double mean_tiled(const state_t *state, const double *obs)  { return mean_layout(state, obs); }
 
 cplx_t matel_diag_pure(const state_t *bra, const state_t *ket, const double *obs) {
+    orkan_flush();
     const size_t dim = (size_t)1 << bra->qubits;
     const double *dobs = orkan_device_doubles("meas", obs, dim);
     double r[2] = {0.0, 0.0};

@@ -42,6 +42,7 @@ static void sm_run_op(const sm_ctx_t *c, qop_t op, cplx_t *x) {
     view.data = x;
     view.qubits = c->n;
     op(&view);
+    orkan_flush();                               /* the op's gates land before x is read */
     SM_VALIDATE(view.data == x && view.type == PURE && view.qubits == c->n,
                 "an operation replaced, freed or resized the state's storage");
 }
@@ -105,6 +106,7 @@ void sample_matrix(state_t *iota, const double *obs, const sm_channel_t *channel
     SM_VALIDATE(channels && n_channels > 0, "no channels");
     SM_VALIDATE(at < n_channels, "channel index out of range");
     SM_VALIDATE(S, "null output pointer");
+    orkan_flush();
     for (unsigned l = 0; l < n_channels; ++l) {
         SM_VALIDATE(channels[l].n_ops > 0 && channels[l].ops, "a channel without operations");
         for (unsigned m = 0; m < channels[l].n_ops; ++m) SM_VALIDATE(channels[l].ops[m], "null operation");

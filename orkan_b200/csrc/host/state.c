@@ -54,6 +54,7 @@ static int is_device_buffer(const void *p) {
 
 void state_init(state_t *state, const qubit_t qubits, cplx_t **data) {
     ORKAN_VALIDATE("state", state != NULL, "state_init: null state");
+    orkan_flush();
     if (state->data) {
         orkan_free_device(state->data);
         state->data = NULL;
@@ -91,6 +92,7 @@ void state_init(state_t *state, const qubit_t qubits, cplx_t **data) {
 
 void state_free(state_t *state) {
     if (!state) return;
+    orkan_fuse_drop(state->data);
     orkan_free_device(state->data);
     state->data = NULL;
     state->qubits = 0;
@@ -113,6 +115,7 @@ void state_tiled_plus(state_t *state, qubit_t qubits) { state->type = MIXED_TILE
 
 state_t state_cp(const state_t *state) {
     ORKAN_VALIDATE("state", state != NULL && state->data != NULL, "state_cp: null state or data");
+    orkan_flush();
     state_t out = *state;
     const idx_t len = state_len(state);
     out.data = orkan_alloc_state(len);
@@ -130,6 +133,7 @@ state_t state_cp(const state_t *state) {
 /* ---- element access (reference state_pure.c:46-56, state_packed.c:79-104,
  *      state_tiled.c:117-150) --------------------------------------------------- */
 static cplx_t read_elem(const state_t *s, idx_t i) {
+    orkan_flush();
     cplx_t v = 0;
     cudaError_t e = cudaMemcpyAsync(&v, s->data + i, sizeof(cplx_t), cudaMemcpyDeviceToHost,
                                     (cudaStream_t)orkan_stream());
@@ -139,6 +143,7 @@ static cplx_t read_elem(const state_t *s, idx_t i) {
 }
 
 static void write_elem(state_t *s, idx_t i, cplx_t v) {
+    orkan_flush();
     cudaError_t e = cudaMemcpyAsync(s->data + i, &v, sizeof(cplx_t), cudaMemcpyHostToDevice,
                                     (cudaStream_t)orkan_stream());
     if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)orkan_stream());

@@ -124,10 +124,12 @@ class _DeviceArray:
 
 
 def state_view(ork, st):
-    """torch complex128 tensor aliasing a state's device storage."""
+    """torch complex128 tensor aliasing a state's device storage (queued statevector gates
+    are launched first, so the view sees every gate applied so far)."""
     import ctypes as C
 
     import torch
+    ork.lib.orkan_flush()
     count = int(ork.lib.state_len(C.byref(st)))
     return torch.as_tensor(_DeviceArray(int(st.data), count, "<c16"), device="cuda")
 

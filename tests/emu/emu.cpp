@@ -12,6 +12,7 @@
 #include "../../orkan_b200/csrc/cuda/dm_engine.cuh"
 #include "../../orkan_b200/csrc/cuda/dm_phase.cuh"
 #include "../../orkan_b200/csrc/cuda/pure.cuh"
+#include "../../orkan_b200/csrc/cuda/pure_fused.cuh"
 #include "../../orkan_b200/csrc/cuda/qaoa.cuh"
 
 #include <stdint.h>
@@ -404,6 +405,35 @@ int emu_fill(double* data, uint64_t len, double re, double im, unsigned corner_l
     for (idx_t tid = 0; tid < nthr; ++tid) fill_thread(mem, len, c2(re, im), corner_log_tile, corner_dim, tid, nthr);
     return 0;
 }
+
+// A fused run of statevector gates (k_pure_fused): every block of the grid, phase by phase
+// (offset table; per chunk: load, each active gate, store), with a block-local chunk buffer.
+int emu_pure_fused(double* psi, unsigned n, unsigned log_chunk, unsigned ngates, const orkan_fgate_t* gates,
+                   unsigned grid_cap, uint32_t* reads, uint32_t* writes, uint64_t* oob) {
+    FusedPlan P;
+    if (!fused_plan(n, log_chunk, ngates, gates, &P)) return -1;
+    const unsigned nthr = kFuseThreads;
+    const idx_t nch = P.nchunks();
+    const unsigned grid = grid_for(1, nch, grid_cap ? grid_cap : kSms * 4u);
+    EmuMem mem{reinterpret_cast<double2*>(psi), idx_t(1) << n, reads, writes, oob};
+    std::vector<double2> buf(P.chunk());
+    std::vector<idx_t> tab(P.ntab());
+    for (unsigned b = 0; b < grid; ++b) {
+        for (unsigned t = 0; t < nthr; ++t) fused_table(P, tab.data(), t, nthr);
+        for (idx_t ch = b; ch < nch; ch += grid) {
+            const idx_t base = fused_base(P, ch);
+            for (unsigned t = 0; t < nthr; ++t) fused_load(mem, P, tab.data(), base, buf.data(), t, nthr);
+            for (unsigned gi = 0; gi < P.ngates; ++gi) {
+                if (!fused_active(P.g[gi], base)) continue;
+                for (unsigned t = 0; t < nthr; ++t) fused_gate(P, P.g[gi], base, buf.data(), t, nthr);
+            }
+            for (unsigned t = 0; t < nthr; ++t) fused_store(mem, P, tab.data(), base, buf.data(), t, nthr);
+        }
+    }
+    return 0;
+}
+
+unsigned long long emu_fused_need(const orkan_fgate_t* g) { return fused_need(*g); }
 
 // Shared-memory layout of the QAOA pass kernel: 1 when every region is aligned for all
 // chunk sizes 0..13 and ring depths 1, 2, for both cost types.

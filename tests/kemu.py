@@ -20,7 +20,8 @@ LAYOUT = {"pure": 0, "packed": 1, "tiled": 2}
 def build() -> str:
     src = os.path.join(HERE, "emu", "emu.cpp")
     deps = [src] + [os.path.join(HERE, "..", "orkan_b200", "csrc", "cuda", f)
-                    for f in ("common.cuh", "dm_engine.cuh", "dm_phase.cuh", "pure.cuh", "qaoa.cuh")]
+                    for f in ("common.cuh", "dm_engine.cuh", "dm_phase.cuh", "pure.cuh", "pure_fused.cuh", "qaoa.cuh")]
+    deps.append(os.path.join(HERE, "..", "include", "orkan_cu.h"))
     if not os.path.exists(LIB) or any(os.path.getmtime(d) > os.path.getmtime(LIB) for d in deps):
         import subprocess
         cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
@@ -134,6 +135,41 @@ def pure_gate(data, n, name, qubits, theta=None):
                                                                    PURE_OP2[name], _ptr(r), _ptr(w), C.byref(b)))
     return _run(lb.emu_pure_ccx, data, lambda o, r, w, b: (_ptr(o), n, int(qubits[0]), int(qubits[1]),
                                                             int(qubits[2]), _ptr(r), _ptr(w), C.byref(b)))
+
+
+FUSED_OP = dict(PURE_OP1, cx=16, cy=17, cz=18, swap=19, ccx=20)
+
+
+class FGate(C.Structure):
+    """orkan_fgate_t of include/orkan_cu.h."""
+    _fields_ = [("op", C.c_int), ("q", C.c_uint * 3), ("c", C.c_double), ("s", C.c_double)]
+
+
+def fused_gates(gates):
+    """[(name, qubits, theta)] -> an orkan_fgate_t array with the host-computed c, s."""
+    arr = (FGate * len(gates))()
+    for i, (name, qs, th) in enumerate(gates):
+        c = s = 0.0
+        if name in ("rx", "ry", "rz"):
+            c, s = np.cos(th / 2.0), np.sin(th / 2.0)
+        elif name == "p":
+            c, s = np.cos(th), np.sin(th)
+        q = list(qs) + [0] * (3 - len(qs))
+        arr[i] = FGate(FUSED_OP[name], (C.c_uint * 3)(*q), c, s)
+    return arr
+
+
+def pure_fused(data, n, log_chunk, gates, grid_cap=0):
+    arr = fused_gates(gates)
+    return _run(lib().emu_pure_fused, data, lambda o, r, w, b: (_ptr(o), n, log_chunk, len(gates), arr,
+                                                                  grid_cap, _ptr(r), _ptr(w), C.byref(b)))
+
+
+def fused_need(name, qubits):
+    lb = lib()
+    lb.emu_fused_need.restype = C.c_ulonglong
+    arr = fused_gates([(name, qubits, 0.5)])
+    return int(lb.emu_fused_need(arr))
 
 
 def pure_exp_diag(data, n, diag, t):

@@ -5,7 +5,7 @@ runs on the host cores beside the CUDA library on the same initial states, and t
 storage arrays are compared at 1e-12 max-abs:
 
 * 14-qubit tiled and packed density matrices (Dirichlet(1,1,1,1) mixtures of 4 Gaussian
-  states, the single-gate sweep's states): a strided subset of 52 sweep gates covering all
+  states, the single-gate sweep's states): every 4th sweep gate (at least 60) covering all
   18 gate calls, applied in sequence.  The two tiled patterns where the reference's tiled
   backend deviates from its own documented semantics (swap with both qubits >= LOG_TILE_DIM,
   ccx with all three) are compared against the reference's packed backend instead, at 10
@@ -64,7 +64,7 @@ def tiled_defect(name, qs, lt=5):
 @pytest.mark.parametrize("kind", ["tiled", "packed"])
 def test_sweep_subset_14q_against_reference(ork5, ref5, kind):
     n = 14
-    plan = [g for g in W.sweep(n)[::5] if not (kind == "tiled" and tiled_defect(g[0], g[1]))]
+    plan = [g for g in W.sweep(n)[::4] if not (kind == "tiled" and tiled_defect(g[0], g[1]))]
     assert len(plan) >= 50 and len({g[0] for g in plan}) == 18
     st = ork5.state(kind, n)
     W.fill_state_on_device(ork5, st, kind, n, seed=1, log_tile=5)
