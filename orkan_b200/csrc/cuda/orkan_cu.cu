@@ -114,6 +114,37 @@ inline bool layout_ok(int layout, unsigned log_tile) {
 // sub-tile side limit: tiles for the tiled layout, 64 for packed
 inline unsigned ls_max_for(int layout, unsigned log_tile) { return layout == 2 ? log_tile : 6u; }
 
+// Result slots of mean / matel_diag in mapped pinned host memory (per device, allocated
+// on first use): the folding block writes the result there, so a call returns its value
+// after one stream synchronisation, without a device-to-host copy.
+struct MappedOut {
+    double* host = nullptr;
+    double* dev = nullptr;
+};
+std::mutex g_mapped_mu;
+MappedOut g_mapped[64];
+
+int mapped_out(MappedOut* m) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (int)e;
+    if (dev < 0 || dev >= 64) return (int)cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_mapped_mu);
+    if (!g_mapped[dev].host) {
+        void* h = nullptr;
+        if ((e = cudaHostAlloc(&h, 64, cudaHostAllocMapped | cudaHostAllocPortable)) != cudaSuccess) return (int)e;
+        void* d = nullptr;
+        if ((e = cudaHostGetDevicePointer(&d, h, 0)) != cudaSuccess) {
+            cudaFreeHost(h);
+            return (int)e;
+        }
+        g_mapped[dev].host = static_cast<double*>(h);
+        g_mapped[dev].dev = static_cast<double*>(d);
+    }
+    *m = g_mapped[dev];
+    return 0;
+}
+
 struct DevMemC2 {
     const double2* p;
     __device__ __forceinline__ double2 ld(idx_t i) const { return p[i]; }
@@ -336,21 +367,22 @@ int orkan_cu_mean(int layout, unsigned log_tile, const void* data, unsigned n, c
     const idx_t d = idx_t(1) << n;
     // PURE: 4 amplitudes per thread per block at least; DM: one diagonal element per thread
     const unsigned np = grid_for(layout == 0 ? kRedThreads * 4 : kRedThreads, d, kRedBlocks);
-    double* part = static_cast<double*>(scratch_get((np + 1) * sizeof(double)));
+    double* part = static_cast<double*>(scratch_get(np * sizeof(double)));
     if (!part) return (int)cudaErrorMemoryAllocation;
-    double* out = part + np;
+    MappedOut out;
+    int rc = mapped_out(&out);
+    if (rc) return rc;
     const double2* rho = static_cast<const double2*>(data);
     if (layout == 0)
-        k_mean_pure<<<np, kRedThreads, 0, st>>>(rho, obs, d, part, out);
+        k_mean_pure<<<np, kRedThreads, 0, st>>>(rho, obs, d, part, out.dev);
     else if (layout == 1)
-        k_mean_dm<PackedMap><<<np, kRedThreads, 0, st>>>(rho, PackedMap{d}, obs, part, out);
+        k_mean_dm<PackedMap><<<np, kRedThreads, 0, st>>>(rho, PackedMap{d}, obs, part, out.dev);
     else
-        k_mean_dm<TiledMap><<<np, kRedThreads, 0, st>>>(rho, TiledMap{d, log_tile}, obs, part, out);
-    const int rc = finish_launch();
-    if (rc) return rc;
-    cudaError_t e = cudaMemcpyAsync(result, out, sizeof(double), cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return (int)e;
-    return (int)cudaStreamSynchronize(st);
+        k_mean_dm<TiledMap><<<np, kRedThreads, 0, st>>>(rho, TiledMap{d, log_tile}, obs, part, out.dev);
+    if ((rc = finish_launch())) return rc;
+    if ((rc = (int)cudaStreamSynchronize(st))) return rc;
+    *result = out.host[0];
+    return 0;
 }
 
 int orkan_cu_matel_diag(const void* bra, const void* ket, unsigned n, const double* obs, double* result,
@@ -359,16 +391,18 @@ int orkan_cu_matel_diag(const void* bra, const void* ket, unsigned n, const doub
     cudaStream_t st = as_stream(stream);
     const idx_t d = idx_t(1) << n;
     const unsigned np = grid_for(kRedThreads * 4, d, kRedBlocks);
-    double* part = static_cast<double*>(scratch_get((2 * np + 2) * sizeof(double)));
+    double* part = static_cast<double*>(scratch_get(2 * np * sizeof(double)));
     if (!part) return (int)cudaErrorMemoryAllocation;
-    double* out = part + 2 * np;
-    k_matel_pure<<<np, kRedThreads, 0, st>>>(static_cast<const double2*>(bra), static_cast<const double2*>(ket), obs,
-                                             d, part, out);
-    const int rc = finish_launch();
+    MappedOut out;
+    int rc = mapped_out(&out);
     if (rc) return rc;
-    cudaError_t e = cudaMemcpyAsync(result, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return (int)e;
-    return (int)cudaStreamSynchronize(st);
+    k_matel_pure<<<np, kRedThreads, 0, st>>>(static_cast<const double2*>(bra), static_cast<const double2*>(ket), obs,
+                                             d, part, out.dev);
+    if ((rc = finish_launch())) return rc;
+    if ((rc = (int)cudaStreamSynchronize(st))) return rc;
+    result[0] = out.host[0];
+    result[1] = out.host[1];
+    return 0;
 }
 
 unsigned long long orkan_cu_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }

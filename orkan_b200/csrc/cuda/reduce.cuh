@@ -65,7 +65,10 @@ __device__ __forceinline__ void fold_partials(const double* partial, unsigned np
         acc = block_sum<kRedThreads>(acc, sh);
         if (threadIdx.x == 0) out[c] = acc;
     }
-    if (threadIdx.x == 0) *ticket = 0u;
+    if (threadIdx.x == 0) {
+        __threadfence_system();          // out may be mapped host memory
+        *ticket = 0u;
+    }
 }
 
 // partial[b] = sum over chunk b of obs[x] * |psi_x|^2; the last block folds them into out[0]

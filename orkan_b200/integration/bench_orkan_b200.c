@@ -14,8 +14,21 @@
  *     harness's host clock around a sequence of applies measures completed gates.
  * touch_bytes are the reference's formulas (2 x storage bytes).  available() checks that
  * the storage fits in the device's free memory.
+ *
+ * The Kraus benchmark's vtable (benchmark/include/bench_kraus.h:54-62; the CPU version is
+ * benchmark/src/bench_kraus_orkan.c) is implemented here too when BENCH_B200_KRAUS is
+ * defined: the superoperator is built once at init with kraus_to_superop (not timed) and
+ * apply calls channel_1q.  With BENCH_B200_AS_REFERENCE the vtables are also exported under
+ * the reference's own names (orkan_tiled_backend, orkan_packed_backend and the
+ * kraus_orkan_* pair), so the reference's unmodified bench_main.c / bench_kraus_main.c,
+ * linked with this file instead of bench_orkan.c / bench_kraus_orkan.c, run their
+ * "orkan" rows on the B200.
  */
+#ifdef BENCH_B200_KRAUS
+#include "bench_kraus.h"
+#else
 #include "bench.h"
+#endif
 
 #include <cuda_runtime.h>
 
@@ -143,3 +156,85 @@ const bench_backend_t orkan_b200_packed_backend = {
     .touch_bytes = b200_packed_bytes,
     .available   = b200_packed_available
 };
+
+#ifdef BENCH_B200_AS_REFERENCE
+extern const bench_backend_t orkan_tiled_backend __attribute__((alias("orkan_b200_tiled_backend")));
+extern const bench_backend_t orkan_packed_backend __attribute__((alias("orkan_b200_packed_backend")));
+#endif
+
+#ifdef BENCH_B200_KRAUS
+/* ---- Kraus benchmark ------------------------------------------------------------------ */
+#include "channel.h"
+
+typedef struct {
+    state_t  *state;
+    superop_t sop;
+} b200_kraus_ctx_t;
+
+static void b200_kraus_apply(void *ctx, const qubit_t *pos) {
+    b200_kraus_ctx_t *c = (b200_kraus_ctx_t *)ctx;
+    channel_1q(c->state, &c->sop, pos[0]);
+    orkan_sync();
+}
+
+static void b200_kraus_cleanup(void *ctx) {
+    b200_kraus_ctx_t *c = (b200_kraus_ctx_t *)ctx;
+    state_free(c->state);
+    free(c->state);
+    free(c->sop.data);
+    free(c);
+}
+
+static void *b200_kraus_init(state_type_t type, qubit_t qubits, int n_ops, int tgt_qubits, const cplx_t *ops) {
+    if (tgt_qubits != 1) return NULL;                  /* channel_1q: 1-qubit channels, as the CPU version */
+    b200_kraus_ctx_t *c = calloc(1, sizeof(b200_kraus_ctx_t));
+    if (!c) return NULL;
+    c->state = calloc(1, sizeof(state_t));
+    if (!c->state) { free(c); return NULL; }
+    c->state->type = type;
+    state_init(c->state, qubits, NULL);
+    if (!c->state->data) { free(c->state); free(c); return NULL; }
+    const idx_t len = state_len(c->state);
+    cplx_t *host = calloc(len, sizeof(cplx_t));
+    if (!host) { state_free(c->state); free(c->state); free(c); return NULL; }
+    if (type == MIXED_TILED) bench_init_hermitian_tiled(host, qubits);
+    else bench_init_hermitian_packed(host, qubits);
+    const int rc = orkan_state_upload(c->state, host);
+    free(host);
+    if (rc) { state_free(c->state); free(c->state); free(c); return NULL; }
+    const kraus_t kraus = {(qubit_t)tgt_qubits, (uint64_t)n_ops, (cplx_t *)ops};
+    c->sop = kraus_to_superop(&kraus);
+    return c;
+}
+
+static void *b200_kraus_tiled_init(qubit_t q, int n_ops, int tgt, const cplx_t *ops) {
+    return b200_kraus_init(MIXED_TILED, q, n_ops, tgt, ops);
+}
+static void *b200_kraus_packed_init(qubit_t q, int n_ops, int tgt, const cplx_t *ops) {
+    return b200_kraus_init(MIXED_PACKED, q, n_ops, tgt, ops);
+}
+
+const bench_kraus_backend_t kraus_orkan_b200_tiled_backend = {
+    .name        = "orkan_b200_tiled",
+    .init        = b200_kraus_tiled_init,
+    .apply       = b200_kraus_apply,
+    .cleanup     = b200_kraus_cleanup,
+    .touch_bytes = b200_tiled_bytes,
+    .available   = b200_tiled_available
+};
+
+const bench_kraus_backend_t kraus_orkan_b200_packed_backend = {
+    .name        = "orkan_b200_packed",
+    .init        = b200_kraus_packed_init,
+    .apply       = b200_kraus_apply,
+    .cleanup     = b200_kraus_cleanup,
+    .touch_bytes = b200_packed_bytes,
+    .available   = b200_packed_available
+};
+
+#ifdef BENCH_B200_AS_REFERENCE
+extern const bench_kraus_backend_t kraus_orkan_tiled_backend __attribute__((alias("kraus_orkan_b200_tiled_backend")));
+extern const bench_kraus_backend_t kraus_orkan_packed_backend
+    __attribute__((alias("kraus_orkan_b200_packed_backend")));
+#endif
+#endif /* BENCH_B200_KRAUS */
