@@ -28,6 +28,18 @@ constexpr unsigned kVec = 4;
 
 #define ORKAN_SQRT1_2 0.70710678118654752440
 
+// c x + s y with one explicitly placed rounding pattern: s y rounded, then one fused
+// multiply-add.  Left to the compiler, "c * x + s * y" may be contracted either way, and
+// differently in different kernels; written out, every kernel that applies a gate (the
+// one-gate kernels, the fused runs, the CPU emulator) gives the same bits.
+ORKAN_HD double lin2(double c, double x, double s, double y) {
+#ifdef __CUDA_ARCH__
+    return __fma_rn(c, x, __dmul_rn(s, y));
+#else
+    return fma(c, x, s * y);
+#endif
+}
+
 // Does the op change amplitude a (target bit 0)?
 ORKAN_HD constexpr bool op1_touches_a(int op) {
     return !(op == kOpZ || op == kOpS || op == kOpSdg || op == kOpT || op == kOpTdg || op == kOpP);
@@ -60,18 +72,18 @@ ORKAN_HD void pair_op(double2& a, double2& b, double c, double s) {
     } else if (OP == kOpTdg) {
         b = c2((b.x + b.y) * ORKAN_SQRT1_2, (b.y - b.x) * ORKAN_SQRT1_2);
     } else if (OP == kOpP) {
-        b = c2(c * b.x - s * b.y, s * b.x + c * b.y);
+        b = c2(lin2(c, b.x, -s, b.y), lin2(c, b.y, s, b.x));
     } else if (OP == kOpRx) {
-        const double2 na = cadd(cscale(a, c), c2(s * b.y, -s * b.x));
-        const double2 nb = cadd(c2(s * a.y, -s * a.x), cscale(b, c));
+        const double2 na = c2(lin2(c, a.x, s, b.y), lin2(c, a.y, -s, b.x));
+        const double2 nb = c2(lin2(c, b.x, s, a.y), lin2(c, b.y, -s, a.x));
         a = na; b = nb;
     } else if (OP == kOpRy) {
-        const double2 na = csub(cscale(a, c), cscale(b, s));
-        const double2 nb = cadd(cscale(a, s), cscale(b, c));
+        const double2 na = c2(lin2(c, a.x, -s, b.x), lin2(c, a.y, -s, b.y));
+        const double2 nb = c2(lin2(c, b.x, s, a.x), lin2(c, b.y, s, a.y));
         a = na; b = nb;
     } else if (OP == kOpRz) {
-        a = c2(c * a.x + s * a.y, c * a.y - s * a.x);
-        b = c2(c * b.x - s * b.y, c * b.y + s * b.x);
+        a = c2(lin2(c, a.x, s, a.y), lin2(c, a.y, -s, a.x));
+        b = c2(lin2(c, b.x, -s, b.y), lin2(c, b.y, s, b.x));
     }
 }
 
