@@ -51,14 +51,14 @@ def parse_args():
     ap.add_argument("--batch-instances", type=int, default=4096, help="instances of the batched QAOA leg (0: skip)")
     ap.add_argument("--batch-check", type=int, default=-1,
                     help="batch instances checked against the per-call path (-1: every instance)")
-    ap.add_argument("--surrogate-pairs", type=int, default=8192,
-                    help="training pairs of the surrogate leg (65536: the full configuration; 0: skip)")
+    ap.add_argument("--surrogate-pairs", type=int, default=65536,
+                    help="training pairs of the surrogate leg (65536: the configured size; 0: skip)")
     ap.add_argument("--circuit-gates", type=int, default=200,
                     help="gates of the fused-circuit leg on the PURE statevector (0: skip)")
     ap.add_argument("--channel-qubits", type=int, default=13,
                     help="density-matrix qubits of the Kraus-channel leg (0: skip)")
-    ap.add_argument("--noisy-pairs", type=int, default=0,
-                    help="training pairs of the noisy (density-matrix) surrogate leg (0: skip)")
+    ap.add_argument("--noisy-pairs", type=int, default=4096,
+                    help="training pairs of the noisy (12 q density-matrix) surrogate leg (0: skip)")
     return ap.parse_args()
 
 

@@ -248,7 +248,7 @@ def _main(argv=None):
     bt = QaoaBatch(ork, [a.qubits] * a.count, edges, None, a.p, f64_costs=a.f64)
     if a.chunk:
         import torch
-        key = f"{torch.cuda.get_device_name()}|n{a.qubits}|p{a.p}|{'f64' if a.f64 else 'u8'}"
+        key = f"{torch.cuda.get_device_name()}|n{a.qubits}|p{a.p}|{'f64' if a.f64 else 'u8'}|v2"
         fd, path = tempfile.mkstemp(suffix=".json")
         with os.fdopen(fd, "w") as f:
             f.write(json.dumps({key: {"C": a.chunk, "threads": a.threads, "ring": a.ring}}) + "\n")

@@ -102,18 +102,37 @@ struct GateFactor {
 };
 
 // exp_diag: tab[x] = (cos(diag[x] t), sin(diag[x] t)); the factor e^{-i(d_r - d_c)t} is
-// formed as in the reference: f_re = cr*cc + sr*sc, f_im = -sr*cc + cr*sc.
+// formed as in the reference: f_re = cr*cc + sr*sc, f_im = -sr*cc + cr*sc.  The S row and S
+// column entries an item needs are staged in shared memory once per item (kStaged), so the
+// element loop reads the state and two shared-memory entries instead of the table.
 template <class MemR2>
 struct TableFactor {
     MemR2 tab;
+    static constexpr bool kStaged = true;
     ORKAN_HD bool item_active(idx_t, idx_t, unsigned) const { return true; }
-    ORKAN_HD bool factor(idx_t r, idx_t c, double2* f) const {
-        const double2 pr = tab.ld(r), pc = tab.ld(c);
+    ORKAN_HD static void combine(double2 pr, double2 pc, double2* f) {
         f->x = pr.x * pc.x + pr.y * pc.y;
         f->y = -pr.y * pc.x + pr.x * pc.y;
+    }
+    ORKAN_HD bool factor(idx_t r, idx_t c, double2* f) const {
+        combine(tab.ld(r), tab.ld(c), f);
         return true;
     }
+    // srow[i] = tab[R + i], scol[j] = tab[C + j] for i, j < S
+    ORKAN_HD void stage(idx_t R, idx_t C, unsigned S, double2* srow, double2* scol, unsigned tid,
+                        unsigned nthr) const {
+        for (unsigned i = tid; i < 2 * S; i += nthr) {
+            if (i < S) srow[i] = tab.ld(R + i);
+            else scol[i - S] = tab.ld(C + i - S);
+        }
+    }
 };
+
+// Factors without staged entries.
+template <class F>
+struct PhaseStaged { static constexpr bool value = false; };
+template <class M>
+struct PhaseStaged<TableFactor<M>> { static constexpr bool value = true; };
 
 // Apply rho' = f * rho  (complex product written out as the reference does:
 // re' = f_re*re - f_im*im, im' = f_re*im + f_im*re).
@@ -133,9 +152,23 @@ ORKAN_HD void tri_unrank_fast(idx_t w, idx_t* u, idx_t* v) {
     *v = w - uu * (uu + 1) / 2;
 }
 
+// Staging phase of item w for staged factors (all threads; a barrier follows).
+template <class Factor>
+ORKAN_HD void dm_phase_stage(const PhaseGeom& g, const Factor& fac, idx_t w, double2* srow, double2* scol,
+                             unsigned tid, unsigned nthr) {
+    if constexpr (PhaseStaged<Factor>::value) {
+        idx_t u, v;
+        tri_unrank_fast(w, &u, &v);
+        fac.stage(u << g.ls, v << g.ls, 1u << g.ls, srow, scol, tid, nthr);
+    } else {
+        (void)g; (void)fac; (void)w; (void)srow; (void)scol; (void)tid; (void)nthr;
+    }
+}
+
 template <class Map, class Mem, class Factor>
 ORKAN_HD void dm_phase_item(const Mem& mem, const Map& map, const PhaseGeom& g, const Factor& fac,
-                            idx_t w, unsigned tid, unsigned nthr) {
+                            idx_t w, unsigned tid, unsigned nthr, const double2* srow = nullptr,
+                            const double2* scol = nullptr) {
     idx_t u, v;
     tri_unrank_fast(w, &u, &v);
     const unsigned ls = g.ls, S = 1u << ls;
@@ -163,7 +196,8 @@ ORKAN_HD void dm_phase_item(const Mem& mem, const Map& map, const PhaseGeom& g, 
             unsigned i, j;
             if (Map::kRowContig) { i = p; j = line; } else { i = line; j = p; }
             if (diag && i <= j) continue;
-            if (!fac.factor(R + i, C + j, &f[k])) continue;
+            if constexpr (PhaseStaged<Factor>::value) Factor::combine(srow[i], scol[j], &f[k]);
+            else if (!fac.factor(R + i, C + j, &f[k])) continue;
             act[k] = true;
             ij[k] = (i << 16) | j;
             addr[k] = Map::kRowContig ? base + (idx_t)line * gcol - (idx_t)((line * (line - 1)) >> 1) + p
@@ -183,8 +217,15 @@ ORKAN_HD void dm_phase_item(const Mem& mem, const Map& map, const PhaseGeom& g, 
 #ifdef __CUDACC__
 template <class Map, class Factor>
 __global__ void __launch_bounds__(kPhaseThreads) k_dm_phase(DevMem mem, Map map, PhaseGeom g, Factor fac) {
-    for (idx_t w = blockIdx.x; w < g.items; w += gridDim.x)
-        dm_phase_item(mem, map, g, fac, w, threadIdx.x, blockDim.x);
+    __shared__ double2 srow[32], scol[32];
+    for (idx_t w = blockIdx.x; w < g.items; w += gridDim.x) {
+        if constexpr (PhaseStaged<Factor>::value) {
+            __syncthreads();                         // the previous item's entries are read
+            dm_phase_stage(g, fac, w, srow, scol, threadIdx.x, blockDim.x);
+            __syncthreads();
+        }
+        dm_phase_item(mem, map, g, fac, w, threadIdx.x, blockDim.x, srow, scol);
+    }
 }
 #endif
 

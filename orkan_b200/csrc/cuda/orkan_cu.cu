@@ -178,7 +178,7 @@ int orkan_cu_fill(int layout, unsigned log_tile, void* data, unsigned n, double 
     } else {
         return (int)cudaErrorInvalidValue;
     }
-    const unsigned grid = grid_for(kPureThreads * 4, len, (unsigned)sm_count() * 8u);
+    const unsigned grid = grid_for(kPureThreads * 4, len, kFullGrid);
     k_fill<<<grid, kPureThreads, 0, as_stream(stream)>>>(DevMem{static_cast<double2*>(data)}, len, c2(re, im), clt,
                                                          cdim);
     return finish_launch();
@@ -187,7 +187,7 @@ int orkan_cu_fill(int layout, unsigned log_tile, void* data, unsigned n, double 
 int orkan_cu_pure_gate1(void* psi, unsigned n, unsigned target, int op, double c, double s, void* stream) {
     if (!psi || n < 1 || n > 62 || target >= n || op < 0 || op >= kNumOp1) return (int)cudaErrorInvalidValue;
     const idx_t npairs = idx_t(1) << (n - 1);
-    const unsigned grid = grid_for(kPureThreads * kVec, npairs, (unsigned)sm_count() * 8u);
+    const unsigned grid = grid_for(kPureThreads * kVec, npairs, kFullGrid);
     DevMem mem{static_cast<double2*>(psi)};
     cudaStream_t st = as_stream(stream);
     switch (op) {
@@ -206,7 +206,7 @@ int orkan_cu_pure_gate2(void* psi, unsigned n, unsigned qa, unsigned qb, int op,
     if (!psi || n < 2 || n > 62 || qa >= n || qb >= n || qa == qb || op < 0 || op >= kNumOp2)
         return (int)cudaErrorInvalidValue;
     const idx_t nq = idx_t(1) << (n - 2);
-    const unsigned grid = grid_for(kPureThreads * kVec, nq, (unsigned)sm_count() * 8u);
+    const unsigned grid = grid_for(kPureThreads * kVec, nq, kFullGrid);
     DevMem mem{static_cast<double2*>(psi)};
     cudaStream_t st = as_stream(stream);
     switch (op) {
@@ -223,7 +223,7 @@ int orkan_cu_pure_ccx(void* psi, unsigned n, unsigned c1, unsigned c2q, unsigned
     if (!psi || n < 3 || n > 62 || c1 >= n || c2q >= n || t >= n || c1 == c2q || c1 == t || c2q == t)
         return (int)cudaErrorInvalidValue;
     const idx_t no = idx_t(1) << (n - 3);
-    const unsigned grid = grid_for(kPureThreads * kVec, no, (unsigned)sm_count() * 8u);
+    const unsigned grid = grid_for(kPureThreads * kVec, no, kFullGrid);
     k_pure_ccx<<<grid, kPureThreads, 0, as_stream(stream)>>>(DevMem{static_cast<double2*>(psi)}, no, c1, c2q, t);
     return finish_launch();
 }
@@ -344,14 +344,14 @@ int orkan_cu_exp_diag(int layout, unsigned log_tile, void* data, unsigned n, con
     cudaStream_t st = as_stream(stream);
     const idx_t d = idx_t(1) << n;
     if (layout == 0) {
-        const unsigned grid = grid_for(kPureThreads * kVec, d, (unsigned)sm_count() * 8u);
+        const unsigned grid = grid_for(kPureThreads * kVec, d, kFullGrid);
         k_pure_exp_diag<<<grid, kPureThreads, 0, st>>>(DevMem{static_cast<double2*>(data)}, DevMemR{diag}, d, t);
         return finish_launch();
     }
     if (!layout_ok(layout, log_tile) || n > 40) return (int)cudaErrorInvalidValue;
     double2* tab = static_cast<double2*>(scratch_get(d * sizeof(double2)));
     if (!tab) return (int)cudaErrorMemoryAllocation;
-    const unsigned grid = grid_for(256, d, (unsigned)sm_count() * 8u);
+    const unsigned grid = grid_for(256, d, kFullGrid);
     k_exp_table<<<grid, 256, 0, st>>>(diag, d, t, tab);
     const int rc = finish_launch();
     if (rc) return rc;

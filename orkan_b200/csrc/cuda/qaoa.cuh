@@ -283,46 +283,61 @@ ORKAN_HD double2 qaoa_phase(CostT c, double gamma, const double2* table) {
     }
 }
 
-// Shared memory of one block: kQaoaRing buffers, each vb[2^C] amplitudes and cw[2^C] cost
-// words (the 4-byte word holding a byte cost, or the FP64 cost), then red[nthr + 32].
+// Shared memory of one block: kQaoaRing buffers, each vb[2^C] amplitudes (padded), the
+// phase table (byte costs) and the costs: FP64 costs one per padded slot (cw), byte costs
+// as a byte array cb copied in runs of 4-16 bytes (see qaoa_cost_index); then red[nthr + 32].
 constexpr unsigned kQaoaRing = 2;
-
-template <class CostT>
-struct QaoaCostWord { typedef uint32_t type; };
-template <>
-struct QaoaCostWord<double> { typedef double type; };
 
 template <class CostT>
 struct QaoaSmem {
     double2* vb;
-    typename QaoaCostWord<CostT>::type* cw;
+    double* cw;            // FP64 costs: one per padded slot
+    uint8_t* cb;           // byte costs (qaoa_cost_index layout)
     double2* tab;          // byte costs: the staged phase table of the pass's phase layer
     double* red;
 };
+
+// Position of slot s's byte cost in cb.  Low and full chunks: s (the chunk's costs are
+// contiguous; chunks of fewer than 4 amplitudes copy the aligned 4-byte word holding them,
+// so their costs start at byte (chunk 2^C) mod 4).  High chunks (s = row + col 2^R): a row's W = 2^lw costs are contiguous in
+// memory, so each row's run is copied whole: cb[row W + col] when W >= 4; for W < 4 the
+// row's 4-byte aligned word is copied to cb[4 row .. 4 row + 3] and the cost sits at byte
+// (c W + col) mod 4 of it (c: the chunk index).
+ORKAN_HD unsigned qaoa_cost_index(unsigned kind, unsigned C, unsigned R, unsigned lw, idx_t chunk, unsigned s) {
+    if (kind == kQaoaFull) return s;
+    if (kind == kQaoaLow) return C >= 2 ? s : (unsigned)((chunk << C) & 3u) + s;
+    const unsigned row = s & ((1u << R) - 1), col = s >> R;
+    if (lw >= 2) return (row << lw) + col;
+    return 4u * row + (unsigned)(((chunk << lw) + col) & 3u);
+}
+
+// Bytes of the byte-cost array of a chunk of 2^C amplitudes: 4 per slot covers high chunks
+// with W < 4 (4 bytes per row, at most 2^C rows), at least 16 for the 16-byte copies of
+// tiny full chunks.
+ORKAN_HD size_t qaoa_cost_bytes(unsigned C) { return C < 2 ? 16u : (size_t(4) << C); }
 
 // Phase-table entries a buffer holds: kQaoaMaxTable for byte costs, none for FP64 costs.
 template <class CostT>
 ORKAN_HD constexpr unsigned qaoa_table_slots() { return std::is_same<CostT, double>::value ? 0u : kQaoaMaxTable; }
 
-// Bytes of one buffer, rounded up to 128 so that every buffer, its cost words and the
-// reduction array after the last buffer keep the alignment of the shared-memory base.
+// Bytes of one buffer, rounded up to 128 so that every buffer, its costs and the reduction
+// array after the last buffer keep the alignment of the shared-memory base.
 template <class CostT>
 ORKAN_HD size_t qaoa_buffer_bytes(unsigned C) {
-    const size_t b = (size_t(16) + sizeof(typename QaoaCostWord<CostT>::type)) * qaoa_padded(C) +
-                     size_t(16) * qaoa_table_slots<CostT>();
+    const size_t cost = std::is_same<CostT, double>::value ? size_t(8) * qaoa_padded(C) : qaoa_cost_bytes(C);
+    const size_t b = size_t(16) * qaoa_padded(C) + size_t(16) * qaoa_table_slots<CostT>() + cost;
     return (b + 127) & ~size_t(127);
 }
 
 // Alignment of every region of a block's shared memory (base aligned to 128 bytes): the
-// 16-byte amplitudes and the asynchronous copies into them, the cost words, the doubles of
-// the reduction.
+// 16-byte amplitudes and the asynchronous copies into them, the costs (16-byte copies of
+// byte runs), the doubles of the reduction.
 template <class CostT>
 ORKAN_HD bool qaoa_smem_aligned(unsigned C, unsigned ring) {
-    const size_t w = sizeof(typename QaoaCostWord<CostT>::type);
     for (unsigned slot = 0; slot < ring; ++slot) {
         const size_t vb = qaoa_buffer_bytes<CostT>(C) * slot, tab = vb + size_t(16) * qaoa_padded(C);
-        const size_t cw = tab + size_t(16) * qaoa_table_slots<CostT>();
-        if (vb % 16 || tab % 16 || cw % w) return false;
+        const size_t cost = tab + size_t(16) * qaoa_table_slots<CostT>();
+        if (vb % 16 || tab % 16 || cost % 16) return false;
     }
     return (qaoa_buffer_bytes<CostT>(C) * ring) % 8 == 0;
 }
@@ -335,19 +350,22 @@ ORKAN_HD QaoaSmem<CostT> qaoa_smem_at(unsigned char* base, unsigned C, unsigned 
     QaoaSmem<CostT> S;
     unsigned char* b = base + qaoa_buffer_bytes<CostT>(C) * slot;
     S.vb = reinterpret_cast<double2*>(b);
-    // [amplitudes, 16 B each][phase table, 16 B each][cost words]: every region aligned
+    // [amplitudes, 16 B each][phase table, 16 B each][costs]: every region aligned
     S.tab = qaoa_table_slots<CostT>() ? reinterpret_cast<double2*>(b + size_t(16) * qaoa_padded(C)) : nullptr;
-    S.cw = reinterpret_cast<typename QaoaCostWord<CostT>::type*>(
-        b + size_t(16) * (qaoa_padded(C) + qaoa_table_slots<CostT>()));
+    unsigned char* c = b + size_t(16) * (qaoa_padded(C) + qaoa_table_slots<CostT>());
+    S.cw = std::is_same<CostT, double>::value ? reinterpret_cast<double*>(c) : nullptr;
+    S.cb = std::is_same<CostT, double>::value ? nullptr : reinterpret_cast<uint8_t*>(c);
     S.red = reinterpret_cast<double*>(base + qaoa_buffer_bytes<CostT>(C) * ring);
     (void)nthr;
     return S;
 }
 
 // Fill of one work item's buffer: asynchronous copies of its amplitudes (unless the pass
-// starts from |+>) and cost words, slot s = tid, tid + nthr, ... in order, so consecutive
-// threads copy consecutive amplitudes.  Mem::cp16(dst, x) copies amplitude x,
-// CostMem::cpw(dst, x) the cost word of amplitude x.
+// starts from |+>), slot s = tid, tid + nthr, ... in order, so consecutive threads copy
+// consecutive amplitudes, and of its costs: FP64 costs per slot, byte costs in runs of
+// 4-16 bytes (a 16-byte copy holds 16 costs; a high chunk's row holds W costs).
+// Mem::cp16(dst, x) copies amplitude x; CostMem::cpw(dst, x) the FP64 cost of amplitude
+// x; CostMem::cpb(dst, x, bytes) bytes byte costs from amplitude x (x a multiple of bytes).
 template <class CostT, class Mem, class CostMem>
 ORKAN_HD void qaoa_fill(const QaoaPass& P, const QaoaTables& T, const QaoaInst& I, const QaoaPlan& pl, const Mem& psi,
                         const CostMem& cost, idx_t chunk, const QaoaSmem<CostT>& S, unsigned tid, unsigned nthr) {
@@ -356,11 +374,21 @@ ORKAN_HD void qaoa_fill(const QaoaPass& P, const QaoaTables& T, const QaoaInst& 
         const double2* row = T.phase + ((idx_t)I.pos * P.p + (unsigned)P.table_layer) * T.tstride;
         for (unsigned e = tid; e < T.tstride; e += nthr) psi.cpg(S.tab + e, row + e);
     }
+    constexpr bool kBytes = !std::is_same<CostT, double>::value;
     if (P.kind != kQaoaHigh) {                     // contiguous chunk: equally spaced copies
         const idx_t x0 = P.kind == kQaoaLow ? chunk << P.C : 0;
         for (unsigned e = tid; e < cnt; e += nthr) {
             if (!pl.init) psi.cp16(S.vb + qaoa_pad(e), x0 + e);
-            cost.cpw(S.cw + qaoa_pad(e), x0 + e);
+            if constexpr (!kBytes) cost.cpw(S.cw + qaoa_pad(e), x0 + e);
+        }
+        if constexpr (kBytes) {
+            if (cnt >= 16 || P.kind == kQaoaFull) {   // 16 costs per copy (whole 16-byte units)
+                for (unsigned e = 16 * tid; e < cnt || (e == 0 && cnt < 16); e += 16 * nthr)
+                    cost.cpb(S.cb + e, x0 + e, 16);
+            } else if (tid == 0) {                    // a chunk of 1-8 costs: one copy
+                if (cnt >= 4) cost.cpb(S.cb, x0, cnt);
+                else cost.cpb(S.cb, x0 & ~idx_t(3), 4);
+            }
         }
         return;
     }
@@ -369,7 +397,19 @@ ORKAN_HD void qaoa_fill(const QaoaPass& P, const QaoaTables& T, const QaoaInst& 
         const unsigned s = qaoa_high_slot(e, R, lw, 0, 0);
         const idx_t x = qaoa_index(I.n, P.C, P.kind, chunk, s);
         if (!pl.init) psi.cp16(S.vb + qaoa_pad(s), x);
-        cost.cpw(S.cw + qaoa_pad(s), x);
+        if constexpr (!kBytes) cost.cpw(S.cw + qaoa_pad(s), x);
+    }
+    if constexpr (kBytes) {
+        // row r's W costs start at amplitude r 2^C + chunk W: runs of min(W, 16) bytes, or the
+        // row's aligned 4-byte word when W < 4
+        const unsigned W = 1u << lw, run = W >= 16 ? 16u : (W >= 4 ? W : 4u);
+        const unsigned per_row = W >= 16 ? W / 16 : 1u;
+        for (unsigned e = tid; e < (per_row << R); e += nthr) {
+            const unsigned row = e / per_row, k = e % per_row;
+            const idx_t x = ((idx_t)row << P.C) + (chunk << lw) + (idx_t)k * run;
+            if (W >= 4) cost.cpb(S.cb + row * W + k * run, x, run);
+            else cost.cpb(S.cb + 4 * row, x & ~idx_t(3), 4);
+        }
     }
 }
 
@@ -386,7 +426,6 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
     const idx_t xs = qaoa_stride(n, P.C, P.kind, B0);
     const idx_t row = (idx_t)I.pos * P.p;
     const double amp0 = 1.0 / sqrt((double)(idx_t(1) << n));
-    const unsigned x3s = (unsigned)xs & 3u;
     double acc = 0.0;
     const bool high = P.kind == kQaoaHigh;
     const unsigned R = high ? n - P.C : 0u, lw = high ? qaoa_logw(n, P.C) : 0u;
@@ -394,16 +433,12 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
         const unsigned base = high ? qaoa_high_slot(r, R, lw, B0, K) : (r & LOWM) | ((r >> B0) << (B0 + K));
         const unsigned p0 = qaoa_pad(base);
         const idx_t xb = qaoa_index(n, P.C, P.kind, chunk, base);      // slot base | j << B0 is xb + j xs
-        const unsigned x3 = (unsigned)xb & 3u;
-        // cost of element j, read from the staged words where it is used
+        // cost of element j, read from the staged costs where it is used
         auto cost_of = [&](unsigned j) -> CostT {
             if constexpr (std::is_same<CostT, double>::value) {
                 return S.cw[p0 + j * D];
             } else {
-                // byte of amplitude xb + j xs in its word: j moves it only when the group
-                // starts at slot bit 0 of a contiguous chunk (xs = 1)
-                const unsigned sh = (B0 == 0 && x3s) ? 8u * ((x3 + j) & 3u) : 8u * x3;
-                return (CostT)((S.cw[p0 + j * D] >> sh) & 0xffu);
+                return S.cb[qaoa_cost_index(P.kind, P.C, R, lw, chunk, base | (j << B0))];
             }
         };
         double2 v[NV];
@@ -548,9 +583,15 @@ struct QaoaDevCost<double> {
 template <>
 struct QaoaDevCost<uint8_t> {
     const uint8_t* p;            // allocated in whole 16-byte units
-    __device__ __forceinline__ void cpw(uint32_t* dst, idx_t i) const {
+    // `bytes` (4, 8 or 16) costs from amplitude i (a multiple of bytes) to dst
+    __device__ __forceinline__ void cpb(uint8_t* dst, idx_t i, unsigned bytes) const {
         const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(p + (i & ~idx_t(3))) : "memory");
+        if (bytes == 16)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(p + i) : "memory");
+        else if (bytes == 8)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(p + i) : "memory");
+        else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(p + i) : "memory");
     }
 };
 __device__ __forceinline__ void qaoa_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }

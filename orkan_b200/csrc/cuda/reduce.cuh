@@ -18,7 +18,7 @@
 namespace orkan {
 
 constexpr unsigned kRedThreads = 256;
-constexpr unsigned kRedBlocks = 1184;      // fixed number of partial sums
+constexpr unsigned kRedBlocks = 4736;      // fixed number of partial sums (32 per SM of B200)
 
 #ifdef __CUDACC__
 template <unsigned NT>

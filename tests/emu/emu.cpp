@@ -85,8 +85,8 @@ struct EmuMemC2 {
     }
 };
 
-// Cost vector accessor of the QAOA fill: the FP64 cost of amplitude i, or the 4-byte word
-// holding byte cost i (len counts the allocated bytes, whole 16-byte units).
+// Cost vector accessor of the QAOA fill: the FP64 cost of amplitude i, or runs of byte
+// costs (len counts the allocated bytes, whole 16-byte units).
 template <class CostT>
 struct EmuCost {
     const CostT* p;
@@ -96,12 +96,10 @@ struct EmuCost {
         if (i >= len) { ++*oob; return; }
         *dst = (double)p[i];
     }
-    void cpw(uint32_t* dst, idx_t i) const {
-        const idx_t a = i & ~idx_t(3);
-        if (a + 4 > len) { ++*oob; return; }
-        uint32_t w;
-        memcpy(&w, reinterpret_cast<const uint8_t*>(p) + a, 4);
-        *dst = w;
+    // byte costs: `bytes` costs from i (a multiple of bytes), within the allocated bytes
+    void cpb(uint8_t* dst, idx_t i, unsigned bytes) const {
+        if ((bytes != 4 && bytes != 8 && bytes != 16) || i % bytes || i + bytes > len) { ++*oob; return; }
+        memcpy(dst, reinterpret_cast<const uint8_t*>(p) + i, bytes);
     }
 };
 
@@ -160,11 +158,14 @@ void run_phase(int layout, unsigned log_tile, const EmuMem& mem, unsigned n, con
     const PhaseGeom g = phase_geometry(n, layout == 2 ? log_tile : 5u);
     const unsigned grid = grid_for(1, g.items, kSms * 32u);
     for (unsigned b = 0; b < grid; ++b)
-        for (idx_t w = b; w < g.items; w += grid)
+        for (idx_t w = b; w < g.items; w += grid) {
+            double2 srow[32], scol[32];
+            for (unsigned t = 0; t < kPhaseThreads; ++t) dm_phase_stage(g, fac, w, srow, scol, t, kPhaseThreads);
             for (unsigned t = 0; t < kPhaseThreads; ++t) {
-                if (layout == 1) dm_phase_item(mem, PackedMap{idx_t(1) << n}, g, fac, w, t, kPhaseThreads);
-                else dm_phase_item(mem, TiledMap{idx_t(1) << n, log_tile}, g, fac, w, t, kPhaseThreads);
+                if (layout == 1) dm_phase_item(mem, PackedMap{idx_t(1) << n}, g, fac, w, t, kPhaseThreads, srow, scol);
+                else dm_phase_item(mem, TiledMap{idx_t(1) << n, log_tile}, g, fac, w, t, kPhaseThreads, srow, scol);
             }
+        }
 }
 
 
