@@ -6,7 +6,9 @@
  * streams are cudaStream_t passed as void* (NULL = the legacy default stream).
  * Every function enqueues its kernel(s) on the stream and returns 0, or a nonzero
  * cudaError_t value (launch failure, invalid argument).  Functions that return a
- * value to the host (orkan_cu_mean, orkan_cu_matel_diag) synchronise the stream.
+ * value to the host (orkan_cu_mean, orkan_cu_matel_diag) return once the value is
+ * available: all work enqueued on the stream before them has then completed (the
+ * reduction's own launch may still be retiring).
  *
  * Layout codes follow state_type_t: 0 = PURE, 1 = MIXED_PACKED, 2 = MIXED_TILED;
  * log_tile is the LOG_TILE_DIM of the tiled layout (ignored otherwise).

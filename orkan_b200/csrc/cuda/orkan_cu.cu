@@ -13,6 +13,8 @@
 #include "../../../include/orkan_cu.h"
 
 #include <atomic>
+#include <chrono>
+#include <cstring>
 #include <stdlib.h>
 #include <mutex>
 
@@ -115,15 +117,18 @@ inline bool layout_ok(int layout, unsigned log_tile) {
 inline unsigned ls_max_for(int layout, unsigned log_tile) { return layout == 2 ? log_tile : 6u; }
 
 // Result slots of mean / matel_diag in mapped pinned host memory (per device, allocated
-// on first use): the folding block writes the result there, so a call returns its value
-// after one stream synchronisation, without a device-to-host copy.
+// on first use): the folding block writes the results there, then a sequence number, so the
+// host reads the value as soon as the number appears, without a device-to-host copy and
+// without waiting for the stream to drain.
 struct MappedOut {
     double* host = nullptr;
     double* dev = nullptr;
+    double seq = 0.0;          // last sequence number issued on this device
 };
 std::mutex g_mapped_mu;
 MappedOut g_mapped[64];
 
+// The device's slots and the next sequence number.
 int mapped_out(MappedOut* m) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -138,11 +143,28 @@ int mapped_out(MappedOut* m) {
             cudaFreeHost(h);
             return (int)e;
         }
+        memset(h, 0, 64);
         g_mapped[dev].host = static_cast<double*>(h);
         g_mapped[dev].dev = static_cast<double*>(d);
     }
+    g_mapped[dev].seq += 1.0;
     *m = g_mapped[dev];
     return 0;
+}
+
+// Wait until the reduction's sequence number shows in slot ncomp: poll the mapped slot for up
+// to 20 ms (results of small states arrive within microseconds), then synchronise the stream,
+// which also reports any error of the launch.
+int wait_mapped(const MappedOut& m, unsigned ncomp, cudaStream_t st) {
+    volatile const double* flag = m.host + ncomp;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (unsigned i = 0;; ++i) {
+        if (*flag == m.seq) return 0;
+        if ((i & 255u) == 255u && std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(20)) break;
+    }
+    const int rc = (int)cudaStreamSynchronize(st);
+    if (rc) return rc;
+    return *flag == m.seq ? 0 : (int)cudaErrorUnknown;
 }
 
 struct DevMemC2 {
@@ -374,14 +396,14 @@ int orkan_cu_mean(int layout, unsigned log_tile, const void* data, unsigned n, c
     if (rc) return rc;
     const double2* rho = static_cast<const double2*>(data);
     if (layout == 0)
-        k_mean_pure<<<np, kRedThreads, 0, st>>>(rho, obs, d, part, out.dev);
+        k_mean_pure<<<np, kRedThreads, 0, st>>>(rho, obs, d, part, out.dev, out.seq);
     else if (layout == 1)
-        k_mean_dm<PackedMap><<<np, kRedThreads, 0, st>>>(rho, PackedMap{d}, obs, part, out.dev);
+        k_mean_dm<PackedMap><<<np, kRedThreads, 0, st>>>(rho, PackedMap{d}, obs, part, out.dev, out.seq);
     else
-        k_mean_dm<TiledMap><<<np, kRedThreads, 0, st>>>(rho, TiledMap{d, log_tile}, obs, part, out.dev);
+        k_mean_dm<TiledMap><<<np, kRedThreads, 0, st>>>(rho, TiledMap{d, log_tile}, obs, part, out.dev, out.seq);
     if ((rc = finish_launch())) return rc;
-    if ((rc = (int)cudaStreamSynchronize(st))) return rc;
-    *result = out.host[0];
+    if ((rc = wait_mapped(out, 1, st))) return rc;
+    *result = static_cast<volatile const double*>(out.host)[0];
     return 0;
 }
 
@@ -397,11 +419,11 @@ int orkan_cu_matel_diag(const void* bra, const void* ket, unsigned n, const doub
     int rc = mapped_out(&out);
     if (rc) return rc;
     k_matel_pure<<<np, kRedThreads, 0, st>>>(static_cast<const double2*>(bra), static_cast<const double2*>(ket), obs,
-                                             d, part, out.dev);
+                                             d, part, out.dev, out.seq);
     if ((rc = finish_launch())) return rc;
-    if ((rc = (int)cudaStreamSynchronize(st))) return rc;
-    result[0] = out.host[0];
-    result[1] = out.host[1];
+    if ((rc = wait_mapped(out, 2, st))) return rc;
+    result[0] = static_cast<volatile const double*>(out.host)[0];
+    result[1] = static_cast<volatile const double*>(out.host)[1];
     return 0;
 }
 

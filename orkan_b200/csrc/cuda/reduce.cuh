@@ -54,9 +54,11 @@ __device__ __forceinline__ bool last_block_done(unsigned* ticket) {
     return last;
 }
 
-// out[c] = sum_b partial[b * ncomp + c] in fixed order, by the whole block; resets the ticket.
+// out[c] = sum_b partial[b * ncomp + c] in fixed order, by the whole block; then out[ncomp] =
+// seq, written after the results are visible system-wide (out may be mapped host memory the
+// host polls); resets the ticket.
 __device__ __forceinline__ void fold_partials(const double* partial, unsigned np, unsigned ncomp, double* out,
-                                              unsigned* ticket) {
+                                              unsigned* ticket, double seq) {
     __shared__ double sh[32];
     __threadfence();
     for (unsigned c = 0; c < ncomp; ++c) {
@@ -66,7 +68,9 @@ __device__ __forceinline__ void fold_partials(const double* partial, unsigned np
         if (threadIdx.x == 0) out[c] = acc;
     }
     if (threadIdx.x == 0) {
-        __threadfence_system();          // out may be mapped host memory
+        __threadfence_system();          // the results land before the sequence number
+        volatile double* vs = out + ncomp;
+        *vs = seq;
         *ticket = 0u;
     }
 }
@@ -74,7 +78,7 @@ __device__ __forceinline__ void fold_partials(const double* partial, unsigned np
 // partial[b] = sum over chunk b of obs[x] * |psi_x|^2; the last block folds them into out[0]
 __global__ void __launch_bounds__(kRedThreads) k_mean_pure(const double2* __restrict__ psi,
                                                            const double* __restrict__ obs, idx_t dim,
-                                                           double* __restrict__ partial, double* __restrict__ out) {
+                                                           double* __restrict__ partial, double* __restrict__ out, double seq) {
     __shared__ double sh[32];
     const idx_t chunk = (dim + gridDim.x - 1) / gridDim.x;
     const idx_t begin = (idx_t)blockIdx.x * chunk;
@@ -95,14 +99,14 @@ __global__ void __launch_bounds__(kRedThreads) k_mean_pure(const double2* __rest
     }
     acc = block_sum<kRedThreads>(acc, sh);
     if (threadIdx.x == 0) partial[blockIdx.x] = acc;
-    if (last_block_done(&g_red_ticket[0])) fold_partials(partial, gridDim.x, 1, out, &g_red_ticket[0]);
+    if (last_block_done(&g_red_ticket[0])) fold_partials(partial, gridDim.x, 1, out, &g_red_ticket[0], seq);
 }
 
 // re/im partials of sum_x obs[x] conj(bra_x) ket_x
 __global__ void __launch_bounds__(kRedThreads) k_matel_pure(const double2* __restrict__ bra,
                                                             const double2* __restrict__ ket,
                                                             const double* __restrict__ obs, idx_t dim,
-                                                            double* __restrict__ partial, double* __restrict__ out) {
+                                                            double* __restrict__ partial, double* __restrict__ out, double seq) {
     __shared__ double sh[32];
     const idx_t chunk = (dim + gridDim.x - 1) / gridDim.x;
     const idx_t begin = (idx_t)blockIdx.x * chunk;
@@ -133,7 +137,7 @@ __global__ void __launch_bounds__(kRedThreads) k_matel_pure(const double2* __res
     sre = block_sum<kRedThreads>(sre, sh);
     sim = block_sum<kRedThreads>(sim, sh);
     if (threadIdx.x == 0) { partial[2 * blockIdx.x] = sre; partial[2 * blockIdx.x + 1] = sim; }
-    if (last_block_done(&g_red_ticket[1])) fold_partials(partial, gridDim.x, 2, out, &g_red_ticket[1]);
+    if (last_block_done(&g_red_ticket[1])) fold_partials(partial, gridDim.x, 2, out, &g_red_ticket[1], seq);
 }
 
 // sum_x obs[x] * Re rho_xx over the diagonal of a packed or tiled density matrix:
@@ -141,7 +145,7 @@ __global__ void __launch_bounds__(kRedThreads) k_matel_pure(const double2* __res
 template <class Map>
 __global__ void __launch_bounds__(kRedThreads) k_mean_dm(const double2* __restrict__ rho, Map map,
                                                          const double* __restrict__ obs, double* __restrict__ partial,
-                                                         double* __restrict__ out) {
+                                                         double* __restrict__ out, double seq) {
     __shared__ double sh[32];
     const idx_t chunk = (map.d + gridDim.x - 1) / gridDim.x;
     const idx_t begin = (idx_t)blockIdx.x * chunk;
@@ -161,7 +165,7 @@ __global__ void __launch_bounds__(kRedThreads) k_mean_dm(const double2* __restri
     for (; x < end; x += kRedThreads) acc += __ldg(obs + x) * rho[map.at(x, x)].x;
     acc = block_sum<kRedThreads>(acc, sh);
     if (threadIdx.x == 0) partial[blockIdx.x] = acc;
-    if (last_block_done(&g_red_ticket[2])) fold_partials(partial, gridDim.x, 1, out, &g_red_ticket[2]);
+    if (last_block_done(&g_red_ticket[2])) fold_partials(partial, gridDim.x, 1, out, &g_red_ticket[2], seq);
 }
 #endif
 

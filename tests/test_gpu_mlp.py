@@ -120,8 +120,11 @@ def test_ascent_increases_the_prediction(ork, torch):
 def test_surrogate_search_beats_plain_sweep_and_its_ablation(ork):
     """The network's gain: with the same exact-evaluation budget (half of it the sweep's
     first pairs, the rest re-scored proposals), the surrogate-guided search finds a higher
-    exact <C> than the plain sweep, and than the same trust-region rounds without the
-    network (starts scored as drawn)."""
+    exact <C> than the plain sweep, and -- over eight seeds of the candidate draws -- than the
+    same trust-region rounds without the network (candidates scored as drawn): a mean gain of
+    at least 0.005 and a win in at least five of the eight.  (Measured on B200: gains +0.054,
+    +0.0002, +0.019, +0.027, +0.044, +0.022, -0.035, -0.012; every step is deterministic, so
+    the figures repeat.)"""
     from orkan_b200.batch import erdos_renyi_graph
     from orkan_b200.surrogate import Evaluator, now, plain_sweep, surrogate_search
     rng = np.random.default_rng(21)
@@ -134,12 +137,17 @@ def test_surrogate_search_beats_plain_sweep_and_its_ablation(ork):
     plain_best = float(e.max())
     half = budget // 2
     kw = dict(target=np.inf, clock=now, rounds=8, proposals=512)
-    best, _, stats = surrogate_search(ork, ev, p, g[:half], b[:half], e[:half], rng=np.random.default_rng(2), **kw)
-    best_abl, _, _ = surrogate_search(ork, ev, p, g[:half], b[:half], e[:half], rng=np.random.default_rng(2),
-                                      use_network=False, **kw)
-    assert half + 512 * stats["rounds"] <= budget
-    assert best > plain_best + 1e-3, (best, plain_best)
-    assert best > best_abl, (best, best_abl)
+    gains = []
+    for seed in range(2, 10):
+        best, _, stats = surrogate_search(ork, ev, p, g[:half], b[:half], e[:half],
+                                          rng=np.random.default_rng(seed), **kw)
+        best_abl, _, _ = surrogate_search(ork, ev, p, g[:half], b[:half], e[:half],
+                                          rng=np.random.default_rng(seed), use_network=False, **kw)
+        assert half + 512 * stats["rounds"] <= budget
+        assert best > plain_best + 1e-3, (best, plain_best)
+        gains.append(best - best_abl)
+    assert np.mean(gains) >= 0.005, gains
+    assert sum(x > 0 for x in gains) >= 5, gains
     # the proposals' exact values are the FP64 simulator's: spot-check one against the oracle
     cost = R.maxcut_cost(n, edges, w)
     gg, bb = rng.uniform(0, np.pi, (1, p)), rng.uniform(0, np.pi / 2, (1, p))
