@@ -261,12 +261,18 @@ int orkan_cu_pure_fused(void* psi, unsigned n, unsigned log_chunk, unsigned ngat
         cudaFuncSetAttribute(k_pure_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
         attr.store(true, std::memory_order_relaxed);
     }
+    // threads per block: 256, or 128 (twice the blocks per SM) through the tuning knob
+    // ORKAN_FUSE_THREADS, read once
+    static const unsigned nt = [] {
+        const char* e = getenv("ORKAN_FUSE_THREADS");
+        return (e && atoi(e) == 128) ? 128u : kFuseThreads;
+    }();
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pure_fused, kFuseThreads, smem) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pure_fused, (int)nt, smem) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;
     const unsigned grid = grid_for(1, plan.nchunks(), (unsigned)(sm_count() * per_sm));
-    k_pure_fused<<<grid, kFuseThreads, smem, as_stream(stream)>>>(DevMem{static_cast<double2*>(psi)}, plan);
+    k_pure_fused<<<grid, nt, smem, as_stream(stream)>>>(DevMem{static_cast<double2*>(psi)}, plan);
     return finish_launch();
 }
 

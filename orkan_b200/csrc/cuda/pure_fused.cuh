@@ -5,6 +5,10 @@
 // gate_pure.c:282-434).  Here a run of gates is applied chunk by chunk: a chunk is the set of
 // 2^C amplitudes whose indices differ only in C chosen "local" qubits, it is loaded into
 // shared memory once, every gate of the run is applied to it there, and it is stored once.
+// Inside the chunk the run is cut into stages: a stage holds consecutive gates whose mixed
+// qubits fit a group of 4 local qubits; every thread takes the 16 amplitudes of a set that
+// differ only in the group's qubits into registers, applies all of the stage's gates there,
+// and puts them back, so the shared memory is read and written once per stage, not per gate.
 //
 // * A gate can join a run when the qubits it mixes are local: the target of X, Y, H, Hy, Rx,
 //   Ry, CX, CY and CCX, both qubits of SWAP.  Controls and diagonal gates (Z, S, Sdg, T, Tdg,
@@ -32,6 +36,7 @@ constexpr unsigned kFuseMaxGates = 48;   // gates of one fused launch
 constexpr unsigned kFuseMaxLog = 12;     // chunk of at most 2^12 amplitudes (64 KB)
 constexpr unsigned kFuseThreads = 256;
 constexpr unsigned kFuseVec = 8;         // loads a thread issues before it stores any
+constexpr unsigned kFuseGroup = 3;       // local qubits of a register stage (8 amplitudes)
 
 enum FKind : unsigned char {
     kFMix = 0,    // pair_op<op> on (bit t clear, bit t set) where the local controls are set
@@ -43,6 +48,8 @@ enum FKind : unsigned char {
 
 struct FGate {
     unsigned char kind, op, t, a;
+    unsigned char rt, ra;      // kFMix / kFSwap: positions of t and a in the stage's group
+    unsigned char pad_[2];
     unsigned lmask;            // local control bits (chunk index)
     unsigned long long gmask;  // the gate acts on a chunk only when all these global bits are set
     unsigned long long gbit;   // kFScale Rz: the global bit that picks the |0> or |1> factor
@@ -54,10 +61,15 @@ struct FusedPlan {
     unsigned ngates;
     unsigned long long nlmask; // global bits that are not local (the chunk id's bits)
     unsigned char lq[kFuseMaxLog];   // global position of local bit i (ascending)
+    unsigned K;                // qubits of a stage's group: min(kFuseGroup, C)
+    unsigned nstages;
+    unsigned char st_first[kFuseMaxGates + 1];     // first gate of stage s; st_first[nstages] = ngates
+    unsigned char st_g[kFuseMaxGates][kFuseGroup]; // local bits of stage s's group, ascending
     FGate g[kFuseMaxGates];
     ORKAN_HD unsigned chunk() const { return 1u << C; }
     ORKAN_HD idx_t nchunks() const { return idx_t(1) << (n - C); }
     ORKAN_HD unsigned ntab() const { return 1u << (C - m); }
+    ORKAN_HD unsigned sets() const { return 1u << (C - K); }
 };
 
 // Global qubits a gate mixes (must be local) as a bit mask; ~0 for an unknown op.
@@ -158,8 +170,48 @@ inline bool fused_plan(unsigned n, unsigned C, unsigned ngates, const orkan_fgat
             default: return false;
         }
     }
+    // stages: consecutive gates whose mixed local bits fit a group of K bits; a group with
+    // fewer is filled with the lowest other local bits
+    P->K = C < kFuseGroup ? C : kFuseGroup;
+    P->nstages = 0;
+    unsigned cur = 0;
+    auto close = [&](unsigned first, unsigned last) {
+        for (unsigned b = 0; b < C && popc64(cur) < P->K; ++b) cur |= 1u << b;
+        unsigned char* gb = P->st_g[P->nstages];
+        unsigned k = 0;
+        for (unsigned b = 0; b < C; ++b)
+            if ((cur >> b) & 1u) gb[k++] = (unsigned char)b;
+        for (; k < kFuseGroup; ++k) gb[k] = 0;
+        for (unsigned gi = first; gi < last; ++gi) {
+            FGate& f = P->g[gi];
+            f.rt = f.ra = 0;
+            for (unsigned r = 0; r < P->K; ++r) {
+                if (gb[r] == f.t) f.rt = (unsigned char)r;
+                if (gb[r] == f.a) f.ra = (unsigned char)r;
+            }
+        }
+        P->st_first[P->nstages++] = (unsigned char)first;
+        cur = 0;
+    };
+    unsigned first = 0;
+    for (unsigned gi = 0; gi < ngates; ++gi) {
+        const FGate& f = P->g[gi];
+        const unsigned need = f.kind == kFMix ? (1u << f.t) : f.kind == kFSwap ? ((1u << f.t) | (1u << f.a)) : 0u;
+        if (popc64(cur | need) > P->K) {
+            close(first, gi);
+            first = gi;
+        }
+        cur |= need;
+    }
+    close(first, ngates);
+    P->st_first[P->nstages] = (unsigned char)ngates;
     return true;
 }
+
+// Shared-memory slot of chunk index s: the low 3 bits XORed with the three 3-bit fields above
+// them, so the 8 lanes of a quarter warp that differ in bits of distinct residues mod 3 (and
+// any 8 consecutive indices) hit distinct 16-byte bank groups.
+ORKAN_HD unsigned fused_phys(unsigned s) { return s ^ (((s >> 3) ^ (s >> 6) ^ (s >> 9)) & 7u); }
 
 // Global index of the chunk's amplitude 0: the chunk id's bits deposited on the non-local bits.
 ORKAN_HD idx_t fused_base(const FusedPlan& P, idx_t chunk) {
@@ -202,7 +254,7 @@ ORKAN_HD void fused_load(const Mem& mem, const FusedPlan& P, const idx_t* tab, i
 #pragma unroll
         for (unsigned u = 0; u < kFuseVec; ++u) {
             const unsigned j = j0 + u * nthr;
-            if (j < N) buf[j] = v[u];
+            if (j < N) buf[fused_phys(j)] = v[u];
         }
     }
 }
@@ -211,107 +263,178 @@ template <class Mem>
 ORKAN_HD void fused_store(const Mem& mem, const FusedPlan& P, const idx_t* tab, idx_t base, const double2* buf,
                           unsigned tid, unsigned nthr) {
     const unsigned N = P.chunk();
-    for (unsigned j = tid; j < N; j += nthr) mem.st(base + fused_off(P, tab, j), buf[j]);
+    for (unsigned j = tid; j < N; j += nthr) mem.st(base + fused_off(P, tab, j), buf[fused_phys(j)]);
 }
 
 // Does gate g act on the chunk at base?  (Its non-local controls are all set.)
 ORKAN_HD bool fused_active(const FGate& g, idx_t base) { return (base & g.gmask) == g.gmask; }
 
-template <int OP>
-ORKAN_HD void fused_mix(const FGate& g, double2* buf, unsigned half, unsigned tid, unsigned nthr) {
-    const unsigned bt = 1u << g.t;
-    for (unsigned p = tid; p < half; p += nthr) {
-        const unsigned i0 = (unsigned)insert0(p, g.t);
-        if ((i0 & g.lmask) != g.lmask) continue;
-        double2 a = buf[i0], b = buf[i0 | bt];
-        pair_op<OP>(a, b, g.c, g.s);
-        buf[i0] = a;
-        buf[i0 | bt] = b;
+// ---- register stages -------------------------------------------------------------------
+// v[j] holds the amplitude at chunk index idx[j] = set base | (bit b of j at group bit g[b]).
+
+template <int OP, int RT, int NV>
+ORKAN_HD void reg_mix(double2 (&v)[NV], const unsigned (&idx)[NV], const FGate& g) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j)
+        if (!(j & (1 << RT)) && (idx[j] & g.lmask) == g.lmask) pair_op<OP>(v[j], v[j | (1 << RT)], g.c, g.s);
+}
+
+template <int OP, int NV>
+ORKAN_HD void reg_mix_at(double2 (&v)[NV], const unsigned (&idx)[NV], const FGate& g) {
+    switch (g.rt) {
+        case 0: reg_mix<OP, 0>(v, idx, g); break;
+        case 1: if (NV > 2) reg_mix<OP, (NV > 2 ? 1 : 0)>(v, idx, g); break;
+        case 2: if (NV > 4) reg_mix<OP, (NV > 4 ? 2 : 0)>(v, idx, g); break;
+        default: if (NV > 8) reg_mix<OP, (NV > 8 ? 3 : 0)>(v, idx, g); break;
     }
 }
 
-template <int OP>
-ORKAN_HD void fused_phase(const FGate& g, double2* buf, unsigned half, unsigned tid, unsigned nthr) {
-    const unsigned bt = 1u << g.t;
-    for (unsigned p = tid; p < half; p += nthr) {
-        const unsigned i1 = (unsigned)insert0(p, g.t) | bt;
-        if ((i1 & g.lmask) != g.lmask) continue;
-        double2 a = c2(0.0, 0.0), b = buf[i1];
-        pair_op<OP>(a, b, g.c, g.s);
-        buf[i1] = b;
+// The |1>-half op of a diagonal gate on local bit t (its bit need not be in the group).
+template <int OP, int NV>
+ORKAN_HD void reg_phase(double2 (&v)[NV], const unsigned (&idx)[NV], const FGate& g) {
+    const unsigned need = g.lmask | (1u << g.t);
+#pragma unroll
+    for (int j = 0; j < NV; ++j)
+        if ((idx[j] & need) == need) {
+            double2 a = c2(0.0, 0.0);
+            pair_op<OP>(a, v[j], g.c, g.s);
+        }
+}
+
+// Rz on local bit t: each amplitude takes the |0> or the |1> factor by its bit t (or, on a
+// non-local bit, by the chunk's bit: `one`).
+// The |1> factor is the |0> factor with s negated: (c x + s y, c y - s x) -> (c x - s y, c y + s x),
+// the same roundings as pair_op<kOpRz>.
+template <int NV>
+ORKAN_HD void reg_rz(double2 (&v)[NV], const unsigned (&idx)[NV], const FGate& g, bool local, bool one) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        const double s = (local ? ((idx[j] >> g.t) & 1u) != 0 : one) ? -g.s : g.s;
+        v[j] = c2(lin2(g.c, v[j].x, s, v[j].y), lin2(g.c, v[j].y, -s, v[j].x));
     }
 }
 
-template <int OP>
-ORKAN_HD void fused_scale(const FGate& g, double2* buf, unsigned N, unsigned tid, unsigned nthr) {
-    for (unsigned j = tid; j < N; j += nthr) {
-        double2 a = c2(0.0, 0.0), b = buf[j];
-        pair_op<OP>(a, b, g.c, g.s);
-        buf[j] = b;
+// A diagonal 1-qubit op's |1> factor on every amplitude (a non-local gate whose bits are set).
+template <int OP, int NV>
+ORKAN_HD void reg_scale(double2 (&v)[NV], const FGate& g) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double2 a = c2(0.0, 0.0);
+        pair_op<OP>(a, v[j], g.c, g.s);
     }
 }
 
-// Rz on a non-local bit: every amplitude takes the |0> factor (bit clear) or the |1> factor.
-ORKAN_HD void fused_scale_rz(const FGate& g, double2* buf, unsigned N, bool one, unsigned tid, unsigned nthr) {
-    for (unsigned j = tid; j < N; j += nthr) {
-        double2 a = buf[j], b = buf[j];
-        pair_op<kOpRz>(a, b, g.c, g.s);
-        buf[j] = one ? b : a;
+template <int RT, int RA, int NV>
+ORKAN_HD void reg_swap(double2 (&v)[NV]) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j)
+        if (!(j & (1 << RT)) && !(j & (1 << RA))) {
+            const double2 x = v[j | (1 << RT)];
+            v[j | (1 << RT)] = v[j | (1 << RA)];
+            v[j | (1 << RA)] = x;
+        }
+}
+
+template <int NV>
+ORKAN_HD void reg_swap_at(double2 (&v)[NV], unsigned rt, unsigned ra) {
+    constexpr int K = NV >= 16 ? 4 : NV >= 8 ? 3 : NV >= 4 ? 2 : 1;
+    const unsigned lo = rt < ra ? rt : ra, hi = rt < ra ? ra : rt;
+    if (K < 2) return;
+    switch (lo * 4 + hi) {
+        case 1: reg_swap<0, 1>(v); break;
+        case 2: if (K > 2) reg_swap<0, (K > 2 ? 2 : 1)>(v); break;
+        case 3: if (K > 3) reg_swap<0, (K > 3 ? 3 : 1)>(v); break;
+        case 6: if (K > 2) reg_swap<1, (K > 2 ? 2 : 0)>(v); break;
+        case 7: if (K > 3) reg_swap<1, (K > 3 ? 3 : 0)>(v); break;
+        default: if (K > 3) reg_swap<2, (K > 3 ? 3 : 0)>(v); break;   // (2, 3)
     }
 }
 
-// One gate on the staged chunk (all threads of the block; a barrier follows).
-ORKAN_HD void fused_gate(const FusedPlan& P, const FGate& g, idx_t base, double2* buf, unsigned tid, unsigned nthr) {
-    const unsigned N = P.chunk(), half = N >> 1;
+// One gate of a stage on a thread's registers.
+template <int NV>
+ORKAN_HD void fused_apply(const FGate& g, double2 (&v)[NV], const unsigned (&idx)[NV], idx_t base) {
     switch (g.kind) {
         case kFMix:
             switch (g.op) {
-                case kOpX: fused_mix<kOpX>(g, buf, half, tid, nthr); break;
-                case kOpY: fused_mix<kOpY>(g, buf, half, tid, nthr); break;
-                case kOpH: fused_mix<kOpH>(g, buf, half, tid, nthr); break;
-                case kOpHy: fused_mix<kOpHy>(g, buf, half, tid, nthr); break;
-                case kOpRx: fused_mix<kOpRx>(g, buf, half, tid, nthr); break;
-                default: fused_mix<kOpRy>(g, buf, half, tid, nthr); break;
+                case kOpX: reg_mix_at<kOpX>(v, idx, g); break;
+                case kOpY: reg_mix_at<kOpY>(v, idx, g); break;
+                case kOpH: reg_mix_at<kOpH>(v, idx, g); break;
+                case kOpHy: reg_mix_at<kOpHy>(v, idx, g); break;
+                case kOpRx: reg_mix_at<kOpRx>(v, idx, g); break;
+                default: reg_mix_at<kOpRy>(v, idx, g); break;
             }
             break;
         case kFPhase:
             switch (g.op) {
-                case kOpZ: fused_phase<kOpZ>(g, buf, half, tid, nthr); break;
-                case kOpS: fused_phase<kOpS>(g, buf, half, tid, nthr); break;
-                case kOpSdg: fused_phase<kOpSdg>(g, buf, half, tid, nthr); break;
-                case kOpT: fused_phase<kOpT>(g, buf, half, tid, nthr); break;
-                case kOpTdg: fused_phase<kOpTdg>(g, buf, half, tid, nthr); break;
-                default: fused_phase<kOpP>(g, buf, half, tid, nthr); break;
+                case kOpZ: reg_phase<kOpZ>(v, idx, g); break;
+                case kOpS: reg_phase<kOpS>(v, idx, g); break;
+                case kOpSdg: reg_phase<kOpSdg>(v, idx, g); break;
+                case kOpT: reg_phase<kOpT>(v, idx, g); break;
+                case kOpTdg: reg_phase<kOpTdg>(v, idx, g); break;
+                default: reg_phase<kOpP>(v, idx, g); break;
             }
             break;
         case kFRz:
-            fused_mix<kOpRz>(g, buf, half, tid, nthr);
+            reg_rz(v, idx, g, true, false);
             break;
-        case kFSwap: {
-            const unsigned lo = g.t < g.a ? g.t : g.a, hi = g.t < g.a ? g.a : g.t;
-            const unsigned bt = 1u << g.t, ba = 1u << g.a;
-            for (unsigned p = tid; p < (N >> 2); p += nthr) {
-                const unsigned i00 = (unsigned)insert0(insert0(p, lo), hi);
-                const double2 x = buf[i00 | bt], y = buf[i00 | ba];
-                buf[i00 | bt] = y;
-                buf[i00 | ba] = x;
-            }
+        case kFSwap:
+            reg_swap_at(v, g.rt, g.ra);
             break;
-        }
         default:   // kFScale
             if (g.op == kOpRz) {
-                fused_scale_rz(g, buf, N, (base & g.gbit) != 0, tid, nthr);
+                reg_rz(v, idx, g, false, (base & g.gbit) != 0);
             } else {
                 switch (g.op) {
-                    case kOpZ: fused_scale<kOpZ>(g, buf, N, tid, nthr); break;
-                    case kOpS: fused_scale<kOpS>(g, buf, N, tid, nthr); break;
-                    case kOpSdg: fused_scale<kOpSdg>(g, buf, N, tid, nthr); break;
-                    case kOpT: fused_scale<kOpT>(g, buf, N, tid, nthr); break;
-                    case kOpTdg: fused_scale<kOpTdg>(g, buf, N, tid, nthr); break;
-                    default: fused_scale<kOpP>(g, buf, N, tid, nthr); break;
+                    case kOpZ: reg_scale<kOpZ>(v, g); break;
+                    case kOpS: reg_scale<kOpS>(v, g); break;
+                    case kOpSdg: reg_scale<kOpSdg>(v, g); break;
+                    case kOpT: reg_scale<kOpT>(v, g); break;
+                    case kOpTdg: reg_scale<kOpTdg>(v, g); break;
+                    default: reg_scale<kOpP>(v, g); break;
                 }
             }
             break;
+    }
+}
+
+// Stage s of the run on the staged chunk (all threads of the block; a barrier follows).
+// Thread tid takes sets tid, tid + nthr, ...: the set's 2^K amplitudes go to registers, every
+// gate of the stage whose chunk condition holds is applied, and they go back.
+template <int NV>
+ORKAN_HD void fused_stage_k(const FusedPlan& P, unsigned s, idx_t base, double2* buf, unsigned tid, unsigned nthr) {
+    constexpr int K = NV >= 16 ? 4 : NV >= 8 ? 3 : NV >= 4 ? 2 : 1;
+    unsigned gbit[4];
+    for (int b = 0; b < 4; ++b) gbit[b] = 1u << P.st_g[s][b];
+    const unsigned g0 = P.st_first[s], g1 = P.st_first[s + 1];
+    for (unsigned r = tid; r < P.sets(); r += nthr) {
+        unsigned sb = r;
+        for (int b = 0; b < K; ++b) sb = (unsigned)insert0(sb, P.st_g[s][b]);   // ascending positions
+        double2 v[NV];
+        unsigned idx[NV];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            unsigned o = sb;
+#pragma unroll
+            for (int b = 0; b < K; ++b)
+                if ((j >> b) & 1) o |= gbit[b];
+            idx[j] = o;
+            v[j] = buf[fused_phys(o)];
+        }
+        for (unsigned gi = g0; gi < g1; ++gi) {
+            const FGate& g = P.g[gi];
+            if (fused_active(g, base)) fused_apply(g, v, idx, base);
+        }
+#pragma unroll
+        for (int j = 0; j < NV; ++j) buf[fused_phys(idx[j])] = v[j];
+    }
+}
+
+ORKAN_HD void fused_stage(const FusedPlan& P, unsigned s, idx_t base, double2* buf, unsigned tid, unsigned nthr) {
+    switch (P.K) {
+        case 4: fused_stage_k<(kFuseGroup >= 4 ? 16 : 8)>(P, s, base, buf, tid, nthr); break;
+        case 3: fused_stage_k<8>(P, s, base, buf, tid, nthr); break;
+        case 2: fused_stage_k<4>(P, s, base, buf, tid, nthr); break;
+        default: fused_stage_k<2>(P, s, base, buf, tid, nthr); break;
     }
 }
 
@@ -323,7 +446,7 @@ ORKAN_HD size_t fused_smem_bytes(const FusedPlan& P) {
 #ifdef __CUDACC__
 // Persistent blocks walk the chunks; every gate whose chunk condition holds is applied in
 // shared memory between one load and one store of the chunk.
-__global__ void __launch_bounds__(kFuseThreads) k_pure_fused(DevMem mem, const __grid_constant__ FusedPlan P) {
+__global__ void __launch_bounds__(kFuseThreads, 2) k_pure_fused(DevMem mem, const __grid_constant__ FusedPlan P) {
     extern __shared__ __align__(16) double2 fbuf[];
     idx_t* tab = reinterpret_cast<idx_t*>(fbuf + P.chunk());
     const unsigned tid = threadIdx.x, nthr = blockDim.x;
@@ -334,10 +457,8 @@ __global__ void __launch_bounds__(kFuseThreads) k_pure_fused(DevMem mem, const _
         const idx_t base = fused_base(P, ch);
         fused_load(mem, P, tab, base, fbuf, tid, nthr);
         __syncthreads();
-        for (unsigned gi = 0; gi < P.ngates; ++gi) {
-            const FGate& g = P.g[gi];
-            if (!fused_active(g, base)) continue;        // the same for every thread of the block
-            fused_gate(P, g, base, fbuf, tid, nthr);
+        for (unsigned st = 0; st < P.nstages; ++st) {
+            fused_stage(P, st, base, fbuf, tid, nthr);
             __syncthreads();
         }
         fused_store(mem, P, tab, base, fbuf, tid, nthr);

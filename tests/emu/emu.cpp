@@ -408,7 +408,7 @@ int emu_fill(double* data, uint64_t len, double re, double im, unsigned corner_l
 }
 
 // A fused run of statevector gates (k_pure_fused): every block of the grid, phase by phase
-// (offset table; per chunk: load, each active gate, store), with a block-local chunk buffer.
+// (offset table; per chunk: load, each register stage, store), with a block-local chunk buffer.
 int emu_pure_fused(double* psi, unsigned n, unsigned log_chunk, unsigned ngates, const orkan_fgate_t* gates,
                    unsigned grid_cap, uint32_t* reads, uint32_t* writes, uint64_t* oob) {
     FusedPlan P;
@@ -424,10 +424,8 @@ int emu_pure_fused(double* psi, unsigned n, unsigned log_chunk, unsigned ngates,
         for (idx_t ch = b; ch < nch; ch += grid) {
             const idx_t base = fused_base(P, ch);
             for (unsigned t = 0; t < nthr; ++t) fused_load(mem, P, tab.data(), base, buf.data(), t, nthr);
-            for (unsigned gi = 0; gi < P.ngates; ++gi) {
-                if (!fused_active(P.g[gi], base)) continue;
-                for (unsigned t = 0; t < nthr; ++t) fused_gate(P, P.g[gi], base, buf.data(), t, nthr);
-            }
+            for (unsigned st = 0; st < P.nstages; ++st)
+                for (unsigned t = 0; t < nthr; ++t) fused_stage(P, st, base, buf.data(), t, nthr);
             for (unsigned t = 0; t < nthr; ++t) fused_store(mem, P, tab.data(), base, buf.data(), t, nthr);
         }
     }
@@ -435,6 +433,13 @@ int emu_pure_fused(double* psi, unsigned n, unsigned log_chunk, unsigned ngates,
 }
 
 unsigned long long emu_fused_need(const orkan_fgate_t* g) { return fused_need(*g); }
+
+// Register stages the plan cuts a run into (-1: the run does not fit).
+int emu_fused_stages(unsigned n, unsigned log_chunk, unsigned ngates, const orkan_fgate_t* gates) {
+    FusedPlan P;
+    if (!fused_plan(n, log_chunk, ngates, gates, &P)) return -1;
+    return (int)P.nstages;
+}
 
 // Shared-memory layout of the QAOA pass kernel: 1 when every region is aligned for all
 // chunk sizes 0..13 and ring depths 1, 2, for both cost types.

@@ -165,6 +165,11 @@ def pure_fused(data, n, log_chunk, gates, grid_cap=0):
                                                                   grid_cap, _ptr(r), _ptr(w), C.byref(b)))
 
 
+def fused_stages(n, log_chunk, gates):
+    arr = fused_gates(gates)
+    return int(lib().emu_fused_stages(n, log_chunk, len(gates), arr))
+
+
 def fused_need(name, qubits):
     lb = lib()
     lb.emu_fused_need.restype = C.c_ulonglong

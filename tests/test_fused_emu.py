@@ -111,3 +111,17 @@ def test_queue_cut_respects_the_gate_cap():
     gates = W.random_circuit(n, 100, seed=5)
     runs = check_runs(n, gates, cap=7)
     assert max(len(r) for r in runs) <= 7
+
+
+def test_register_stages_group_the_mixed_qubits():
+    """A stage holds consecutive gates whose mixed local qubits fit a group of three: mixing
+    gates on three distinct qubits and any number of diagonal gates and controls share one
+    stage, a fourth distinct mixed qubit opens the next, and runs of random gates need far
+    fewer stages than gates (each stage is one shared-memory round trip of the chunk)."""
+    n = 12
+    run = [("h", (1,), None), ("t", (9,), None), ("rx", (4,), 0.3), ("cz", (2, 7), None), ("y", (6,), None),
+           ("rz", (11,), 0.2), ("cx", (3, 6), None), ("ccx", (9, 10, 4), None), ("p", (0,), 1.1)]
+    assert kemu.fused_stages(n, 12, run) == 1
+    assert kemu.fused_stages(n, 12, run + [("h", (10,), None)]) == 2
+    gates = W.random_circuit(n, 48, seed=8)
+    assert kemu.fused_stages(n, 12, gates) <= 48 // 3
