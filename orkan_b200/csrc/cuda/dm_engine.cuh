@@ -516,6 +516,18 @@ struct OpSuper1 {
 struct OpSuper2 {
     double2 s[256];
     ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr, unsigned = 3u) const {
+#ifdef __CUDA_ARCH__
+        // the superoperator is read 16 times per group: from shared memory (one broadcast
+        // load per complex entry) rather than from the kernel parameters (every thread writes
+        // the same values, and the engine's barriers separate one item's reads from the next
+        // item's writes)
+        __shared__ double2 ss[256];
+        for (unsigned i = tid; i < 256; i += nthr) ss[i] = s[i];
+        __syncthreads();
+        const double2* sp = ss;
+#else
+        const double2* sp = s;
+#endif
         const unsigned P = g.P(), lq = g.ls + g.h - 2;
         unsigned asc[2] = {g.vbit[0] < g.vbit[1] ? g.vbit[0] : g.vbit[1],
                            g.vbit[0] < g.vbit[1] ? g.vbit[1] : g.vbit[0]};
@@ -533,11 +545,20 @@ struct OpSuper2 {
             for (unsigned r = 0; r < 4; ++r)
                 for (unsigned c = 0; c < 4; ++c) x[4 * r + c] = vb[ri[r] * P + ci[c]];
 #pragma unroll 1
-            for (unsigned m = 0; m < 16; ++m) {
-                double2 acc = c2(0.0, 0.0);
+            for (unsigned r = 0; r < 4; ++r) {                // output row r, two outputs at a time
+                const unsigned rowoff = dm_set_local(rb, r, g.vbit, 2) * P;
 #pragma unroll
-                for (unsigned j = 0; j < 16; ++j) acc = cadd(acc, cmul(s[16 * m + j], x[j]));
-                vb[ri[m >> 2] * P + ci[m & 3]] = acc;
+                for (unsigned c = 0; c < 4; c += 2) {
+                    const unsigned m = 4 * r + c;
+                    double2 acc0 = c2(0.0, 0.0), acc1 = c2(0.0, 0.0);
+#pragma unroll
+                    for (unsigned j = 0; j < 16; ++j) {
+                        acc0 = cadd(acc0, cmul(sp[16 * m + j], x[j]));
+                        acc1 = cadd(acc1, cmul(sp[16 * m + 16 + j], x[j]));
+                    }
+                    vb[rowoff + ci[c]] = acc0;
+                    vb[rowoff + ci[c + 1]] = acc1;
+                }
             }
         }
     }
