@@ -446,7 +446,7 @@ ORKAN_HD size_t fused_smem_bytes(const FusedPlan& P) {
 #ifdef __CUDACC__
 // Persistent blocks walk the chunks; every gate whose chunk condition holds is applied in
 // shared memory between one load and one store of the chunk.
-__global__ void __launch_bounds__(kFuseThreads, 2) k_pure_fused(DevMem mem, const __grid_constant__ FusedPlan P) {
+__global__ void __launch_bounds__(kFuseThreads) k_pure_fused(DevMem mem, const __grid_constant__ FusedPlan P) {
     extern __shared__ __align__(16) double2 fbuf[];
     idx_t* tab = reinterpret_cast<idx_t*>(fbuf + P.chunk());
     const unsigned tid = threadIdx.x, nthr = blockDim.x;
