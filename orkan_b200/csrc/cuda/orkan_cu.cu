@@ -62,7 +62,12 @@ template <class Kern>
 unsigned engine_grid(Kern kern, size_t smem, idx_t items) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        // the dynamic limit leaves room for the kernel's static shared memory (the 2-qubit
+        // superoperator stages its entries there): static + dynamic may not exceed 227 KB
+        cudaFuncAttributes fa;
+        size_t stat = 0;
+        if (cudaFuncGetAttributes(&fa, kern) == cudaSuccess) stat = fa.sharedSizeBytes;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(227 * 1024 - stat));
         attr = true;
     }
     int per_sm = 0;
