@@ -28,11 +28,15 @@ inline unsigned grid_for(idx_t work_per_block_units, idx_t total_units, unsigned
     return (unsigned)g;
 }
 
+// Items (S x S sub-tiles) per block of the phase pass: 1, or 2 / 4 / 8 through the tuning
+// knob ORKAN_PHASE_ITEMS, read once.
+unsigned phase_items_per_block();
+
 // Elementwise phase pass over a packed (layout 1) or tiled (layout 2) density matrix.
 template <class Factor>
 int launch_phase(int layout, unsigned log_tile, void* rho, unsigned n, const Factor& fac, cudaStream_t st) {
     const PhaseGeom g = phase_geometry(n, layout == 2 ? log_tile : 5u);
-    const unsigned grid = grid_for(1, g.items, kFullGrid);
+    const unsigned grid = grid_for(phase_items_per_block(), g.items, kFullGrid);
     DevMem mem{static_cast<double2*>(rho)};
     if (layout == 1) {
         k_dm_phase<PackedMap, Factor><<<grid, kPhaseThreads, 0, st>>>(mem, PackedMap{idx_t(1) << n}, g, fac);

@@ -43,6 +43,15 @@ int finish_launch() {
     return (int)cudaGetLastError();
 }
 
+unsigned phase_items_per_block() {
+    static const unsigned v = [] {
+        const char* e = getenv("ORKAN_PHASE_ITEMS");
+        const int x = e ? atoi(e) : 1;
+        return (x == 2 || x == 4 || x == 8) ? (unsigned)x : 1u;
+    }();
+    return v;
+}
+
 }  // namespace orkan
 
 namespace {
