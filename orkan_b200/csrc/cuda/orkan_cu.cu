@@ -62,8 +62,6 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 std::atomic<unsigned long long> g_engine_test_polls{0};
 std::atomic<unsigned> g_engine_test_drop{0};
 
-struct Complex8 { double2 v[8]; };
-
 inline double2 ld_c(const double* p, unsigned i) { return c2(p[2 * i], p[2 * i + 1]); }
 
 // ---- density-matrix engine dispatch -------------------------------------------------

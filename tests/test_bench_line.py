@@ -1,0 +1,44 @@
+"""Host-side pieces of bench.py's JSON line (CPU only): the workload description both arms
+share, the reference sample (the same fixed gates in the GPU arm's cpu_baseline and in every
+step of the reference arm), the per-class DRAM traffic read from profiles/, and the
+configured sizes of the learned legs."""
+import json
+import os
+
+import bench
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_both_arms_describe_the_same_workload():
+    plan = bench.build_plan(12, 6)
+    cfg = bench.sweep_config(12, 6, plan)
+    assert cfg["gates_per_step"] == len(plan)
+    assert cfg["algorithmic_bytes_per_step"] == sum(e[5] for e in plan)
+    assert "12 q PURE" in cfg["workload"] and "6 q tiled and packed" in cfg["workload"]
+
+
+def test_reference_sample_is_fixed_and_described():
+    plan = bench.build_plan(30, 14)
+    assert len(plan) == 1056
+    txt = bench.sample_text(plan, 16, 7.5)
+    assert f"every {bench.SAMPLE_STRIDE}th gate" in txt and "76 of 1056" in txt
+    assert "30 q PURE, 14 q tiled, 14 q packed" in txt and "OpenMP threads = 16" in txt
+
+
+def test_profiled_traffic_covers_the_sweep_classes():
+    prof = bench.profiled_traffic()
+    with open(os.path.join(ROOT, "profiles", "traffic_per_launch.json")) as f:
+        raw = json.load(f)
+    classes = {bench.kernel_class(kind, name) for kind, _, name, *_ in bench.build_plan(8, 6)}
+    assert classes <= set(prof)
+    for c, (dram, alg) in prof.items():
+        assert raw[c]["kernel"] and 0.8 < dram / alg < 2.0
+
+
+def test_learned_legs_run_at_their_configured_sizes(monkeypatch):
+    import sys
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    a = bench.parse_args()
+    assert a.surrogate_pairs == 65536 and a.noisy_pairs > 0
+    assert a.batch_instances == 4096 and a.batch_check == -1 and a.circuit_gates == 200
