@@ -140,7 +140,7 @@ ORKAN_HD double2 phase_apply(double2 f, double2 v) {
     return c2(f.x * v.x - f.y * v.y, f.x * v.y + f.y * v.x);
 }
 
-constexpr unsigned kPhaseEpt = 8;     // elements per thread per trip: loads issued together
+constexpr unsigned kPhaseEpt = 4;     // elements per thread per trip: loads issued together
 
 // Row u, column v of the lower-triangular item index w = u(u+1)/2 + v (single-precision
 // estimate, corrected exactly in integers).
