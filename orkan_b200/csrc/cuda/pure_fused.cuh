@@ -274,9 +274,16 @@ ORKAN_HD bool fused_active(const FGate& g, idx_t base) { return (base & g.gmask)
 
 template <int OP, int RT, int NV>
 ORKAN_HD void reg_mix(double2 (&v)[NV], const unsigned (&idx)[NV], const FGate& g) {
+    const double c = g.c, s = g.s;
+    if (g.lmask == 0) {                              // no local control: every pair
+#pragma unroll
+        for (int j = 0; j < NV; ++j)
+            if (!(j & (1 << RT))) pair_op<OP>(v[j], v[j | (1 << RT)], c, s);
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < NV; ++j)
-        if (!(j & (1 << RT)) && (idx[j] & g.lmask) == g.lmask) pair_op<OP>(v[j], v[j | (1 << RT)], g.c, g.s);
+        if (!(j & (1 << RT)) && (idx[j] & g.lmask) == g.lmask) pair_op<OP>(v[j], v[j | (1 << RT)], c, s);
 }
 
 template <int OP, int NV>
@@ -403,29 +410,36 @@ ORKAN_HD void fused_apply(const FGate& g, double2 (&v)[NV], const unsigned (&idx
 template <int NV>
 ORKAN_HD void fused_stage_k(const FusedPlan& P, unsigned s, idx_t base, double2* buf, unsigned tid, unsigned nthr) {
     constexpr int K = NV >= 16 ? 4 : NV >= 8 ? 3 : NV >= 4 ? 2 : 1;
-    unsigned gbit[4];
-    for (int b = 0; b < 4; ++b) gbit[b] = 1u << P.st_g[s][b];
+    // element j of a set sits at set base | off[j]; the swizzle is linear over disjoint bits,
+    // so its slot is phys(set base) ^ phys(off[j]), with phys(off[j]) formed once per stage
+    unsigned off[NV], poff[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        unsigned o = 0;
+#pragma unroll
+        for (int b = 0; b < K; ++b)
+            if ((j >> b) & 1) o |= 1u << P.st_g[s][b];
+        off[j] = o;
+        poff[j] = fused_phys(o);
+    }
     const unsigned g0 = P.st_first[s], g1 = P.st_first[s + 1];
     for (unsigned r = tid; r < P.sets(); r += nthr) {
         unsigned sb = r;
         for (int b = 0; b < K; ++b) sb = (unsigned)insert0(sb, P.st_g[s][b]);   // ascending positions
+        const unsigned psb = fused_phys(sb);
         double2 v[NV];
         unsigned idx[NV];
 #pragma unroll
         for (int j = 0; j < NV; ++j) {
-            unsigned o = sb;
-#pragma unroll
-            for (int b = 0; b < K; ++b)
-                if ((j >> b) & 1) o |= gbit[b];
-            idx[j] = o;
-            v[j] = buf[fused_phys(o)];
+            idx[j] = sb | off[j];
+            v[j] = buf[psb ^ poff[j]];
         }
         for (unsigned gi = g0; gi < g1; ++gi) {
             const FGate& g = P.g[gi];
             if (fused_active(g, base)) fused_apply(g, v, idx, base);
         }
 #pragma unroll
-        for (int j = 0; j < NV; ++j) buf[fused_phys(idx[j])] = v[j];
+        for (int j = 0; j < NV; ++j) buf[psb ^ poff[j]] = v[j];
     }
 }
 
