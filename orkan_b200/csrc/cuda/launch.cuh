@@ -28,7 +28,7 @@ inline unsigned grid_for(idx_t work_per_block_units, idx_t total_units, unsigned
     return (unsigned)g;
 }
 
-// Items (S x S sub-tiles) per block of the phase pass: 1, or 2 / 4 / 8 through the tuning
+// Items (S x S sub-tiles) per block of the phase pass: 2, or 1 / 4 / 8 through the tuning
 // knob ORKAN_PHASE_ITEMS, read once.
 unsigned phase_items_per_block();
 

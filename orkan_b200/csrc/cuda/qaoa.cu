@@ -234,13 +234,13 @@ int dalloc(T** p, size_t count) {
     return (int)cudaMalloc(reinterpret_cast<void**>(p), (count ? count : 1) * sizeof(T));
 }
 
-unsigned default_C(unsigned n) { return n <= 12 ? n : n >= 23 ? 13u : std::max(12u, (n + 1) / 2); }
+unsigned default_C(unsigned n) { return n <= 12 ? n : std::max(12u, (n + 1) / 2); }
 bool is_full(const orkan_qaoa* b, unsigned n) { return n <= b->cfg[n].C; }
 
 // Default: 2^12-amplitude chunks, 256 threads (one 16-amplitude set per thread and stage),
-// one buffer, so that two blocks share an SM; 2^13 with 512 threads from 23 qubits (measured
-// 1.7x faster than 2^12 with 128 threads at 24 qubits); instances up to 12 qubits in one full
-// pass.
+// one buffer, so that two blocks share an SM; instances up to 12 qubits in one full pass.
+// Measured on 16 instances (p = 4, byte costs): 21.1 ms per run at 24 qubits against 23.4 ms
+// for 2^13 with 512 threads, 9.6 against 11.6 ms at 23 qubits.
 QaoaCfg default_cfg(unsigned n) {
     QaoaCfg c;
     c.C = default_C(n);
