@@ -504,7 +504,13 @@ struct OpSuper1 {
             for (unsigned m = 0; m < 4; ++m) x[m] = vb[idx[m]];
             for (unsigned m = 0; m < 4; ++m) {
                 double2 acc = c2(0.0, 0.0);
-                for (unsigned j = 0; j < 4; ++j) acc = cadd(acc, cmul(s[4 * m + j], x[j]));
+                for (unsigned j = 0; j < 4; ++j) {          // four FMAs per complex term
+                    const double2 sj = s[4 * m + j];
+                    acc.x = fma(sj.x, x[j].x, acc.x);
+                    acc.x = fma(-sj.y, x[j].y, acc.x);
+                    acc.y = fma(sj.x, x[j].y, acc.y);
+                    acc.y = fma(sj.y, x[j].x, acc.y);
+                }
                 vb[idx[m]] = acc;
             }
         }
@@ -551,10 +557,19 @@ struct OpSuper2 {
                 for (unsigned c = 0; c < 4; c += 2) {
                     const unsigned m = 4 * r + c;
                     double2 acc0 = c2(0.0, 0.0), acc1 = c2(0.0, 0.0);
+                    // complex multiply-add as four FMAs (a product then an add would take six
+                    // FP64 operations per term)
 #pragma unroll
                     for (unsigned j = 0; j < 16; ++j) {
-                        acc0 = cadd(acc0, cmul(sp[16 * m + j], x[j]));
-                        acc1 = cadd(acc1, cmul(sp[16 * m + 16 + j], x[j]));
+                        const double2 s0 = sp[16 * m + j], s1 = sp[16 * m + 16 + j];
+                        acc0.x = fma(s0.x, x[j].x, acc0.x);
+                        acc0.x = fma(-s0.y, x[j].y, acc0.x);
+                        acc0.y = fma(s0.x, x[j].y, acc0.y);
+                        acc0.y = fma(s0.y, x[j].x, acc0.y);
+                        acc1.x = fma(s1.x, x[j].x, acc1.x);
+                        acc1.x = fma(-s1.y, x[j].y, acc1.x);
+                        acc1.y = fma(s1.x, x[j].y, acc1.y);
+                        acc1.y = fma(s1.y, x[j].x, acc1.y);
                     }
                     vb[rowoff + ci[c]] = acc0;
                     vb[rowoff + ci[c + 1]] = acc1;
