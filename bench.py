@@ -242,7 +242,8 @@ def sweep_config(npure: int, nmix: int, plan) -> dict:
                         f"density matrices, {len(plan)} gate applications per step",
             "pure_qubits": npure, "mixed_qubits": nmix, "gates_per_step": len(plan),
             "algorithmic_bytes_per_step": sum(e[5] for e in plan),
-            "l2": "inputs larger than L2 (16 GiB and 2.15 GB states vs 126 MB L2); no flush"}
+            "l2": (f"inputs larger than L2 ({16 * 2 ** npure / 2 ** 30:g} GiB and "
+                   f"{16 * (2 ** nmix) * (2 ** nmix + 1) / 2 / 1e9:.3g} GB states vs 126 MB L2); no flush")}
 
 
 def sample_text(plan, cores, secs=None) -> str:
