@@ -28,7 +28,9 @@ void orkan_sync(void);
  * on the same statevector are applied in one pass over device memory.  Every other call
  * that touches device state launches the queue first, so results seen through the API are
  * those of the gates applied one by one (bit for bit).  Callers that read state_t.data with
- * their own kernels call orkan_flush (or orkan_sync) first.
+ * their own kernels call orkan_flush (or orkan_sync) first, and callers that capture the
+ * library stream into a CUDA graph call orkan_flush before they end the capture (queued
+ * gates are launched at the flush).
  * orkan_set_gate_fusion(k) caps a fused run at k gates (at most 48); k <= 1 launches every
  * gate at once, as the reference applies it.  The initial cap is read from the environment
  * variable ORKAN_GATE_FUSION (default 48).  No counterpart in the reference. */
