@@ -411,6 +411,10 @@ def channels_leg(args, ork, clocks_cls, local):
     n = args.channel_qubits
     chans = W.channel_set(n, seed=3)
     sops = [(label, ork.superop(kr), q) for label, kr, q in chans]
+    import numpy as np
+    rng2 = np.random.default_rng(11)
+    iso, _ = np.linalg.qr(rng2.standard_normal((16, 4)) + 1j * rng2.standard_normal((16, 4)))
+    sop2 = ork.superop([iso[4 * i:4 * i + 4, :] for i in range(4)])
     out = {"metric": "channel GB/s", "unit": "GB/s", "dtype": "f64",
            "config": {"workload": f"{n} q tiled and packed density matrices (Dirichlet(1,1,1,1) mixtures of 4 "
                                   f"Gaussian states): depolarizing p~U[0,0.1], amplitude damping g~U[0,0.2], phase "
@@ -442,6 +446,22 @@ def channels_leg(args, ork, clocks_cls, local):
         out[kind] = {"value": nbytes / (ms * 1e-3) / 1e9, "ms_per_step": ms, "algorithmic_bytes_per_step": nbytes,
                      "frac_of_peak": nbytes / (ms * 1e-3) / 1e9 / peak, "peak_source": peak_kind,
                      "trace_after": ork.mean(st, ones.data_ptr()), "mean": m, "clocks": clocks}
+        # 2-qubit channels (channel_2q): the random 4-Kraus CPTP map on (q, q + 5 mod n) for
+        # every q; every element changes, 64 FP64 FMA per element
+        pairs = [(q, (q + 5) % n) for q in range(n)]
+        for q0, q1 in pairs[:3]:
+            ork.channel_2q(st, sop2, q0, q1)
+        torch.cuda.synchronize()
+        e0.record()
+        for q0, q1 in pairs:
+            ork.channel_2q(st, sop2, q0, q1)
+        e1.record()
+        torch.cuda.synchronize()
+        ms2 = e0.elapsed_time(e1) / len(pairs)
+        b2 = T.gate_bytes(kind, n, "h", (0,), 5)
+        out[kind]["channel_2q"] = {"value": b2 / (ms2 * 1e-3) / 1e9, "us_per_call": ms2 * 1e3,
+                                   "frac_of_peak": b2 / (ms2 * 1e-3) / 1e9 / peak, "calls": len(pairs),
+                                   "trace_after": ork.mean(st, ones.data_ptr())}
         ork.free(st)
     # observables: mean on both layouts above; matel_diag is PURE-only in the reference
     pst, ket = ork.state("pure", n), ork.state("pure", n)

@@ -426,26 +426,41 @@ ORKAN_HD unsigned dm_get_local(unsigned x, const unsigned* vbit, unsigned k) {
 }
 
 // Dense 1-qubit unitary U (row-major u[2*r + c]):  G' = U G U^dagger on 2x2 groups.
+// Bank-conflict-free order of a 2 x 2 group's two columns.  The lanes of a warp share the
+// group row and take consecutive column indices with the gate bit inserted; for a gate bit
+// below 3 the 8 lanes of a quarter warp then fall on only four 16-byte bank groups (every
+// other slot).  Lanes with bit 2 set touch their second column first, which lies on the four
+// other bank groups, so each access instruction of the quarter warp hits eight.
+ORKAN_HD bool dm_swap_cols(unsigned vbq, unsigned lh, unsigned tid) { return vbq < 3 && lh >= 5 && (tid & 4u); }
+
 struct OpMix1 {
     double2 u[4];
     ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr, unsigned = 3u) const {
         const unsigned P = g.P(), lh = g.ls + g.h - 1, vbq = g.vbit[0];
         const unsigned groups = 1u << (2 * lh);
+        const bool sw = dm_swap_cols(vbq, lh, tid);
         for (unsigned t = tid; t < groups; t += nthr) {
             const unsigned r0 = (unsigned)insert0(t >> lh, vbq), c0 = (unsigned)insert0(t & ((1u << lh) - 1), vbq);
             const unsigned r1 = r0 | (1u << vbq), c1 = c0 | (1u << vbq);
-            const double2 x00 = vb[r0 * P + c0], x01 = vb[r0 * P + c1];
-            const double2 x10 = vb[r1 * P + c0], x11 = vb[r1 * P + c1];
+            const unsigned ca = sw ? c1 : c0, cb = sw ? c0 : c1;
+            const double2 y0a = vb[r0 * P + ca], y0b = vb[r0 * P + cb];
+            const double2 y1a = vb[r1 * P + ca], y1b = vb[r1 * P + cb];
+            const double2 x00 = sw ? y0b : y0a, x01 = sw ? y0a : y0b;
+            const double2 x10 = sw ? y1b : y1a, x11 = sw ? y1a : y1b;
             // rows: Y = U X
             const double2 y00 = cadd(cmul(u[0], x00), cmul(u[1], x10));
             const double2 y01 = cadd(cmul(u[0], x01), cmul(u[1], x11));
             const double2 y10 = cadd(cmul(u[2], x00), cmul(u[3], x10));
             const double2 y11 = cadd(cmul(u[2], x01), cmul(u[3], x11));
             // columns: Z = Y U^dagger, Z[i][j] = sum_m Y[i][m] conj(U[j][m])
-            vb[r0 * P + c0] = cadd(cmulc(y00, u[0]), cmulc(y01, u[1]));
-            vb[r0 * P + c1] = cadd(cmulc(y00, u[2]), cmulc(y01, u[3]));
-            vb[r1 * P + c0] = cadd(cmulc(y10, u[0]), cmulc(y11, u[1]));
-            vb[r1 * P + c1] = cadd(cmulc(y10, u[2]), cmulc(y11, u[3]));
+            const double2 z00 = cadd(cmulc(y00, u[0]), cmulc(y01, u[1]));
+            const double2 z01 = cadd(cmulc(y00, u[2]), cmulc(y01, u[3]));
+            const double2 z10 = cadd(cmulc(y10, u[0]), cmulc(y11, u[1]));
+            const double2 z11 = cadd(cmulc(y10, u[2]), cmulc(y11, u[3]));
+            vb[r0 * P + ca] = sw ? z01 : z00;
+            vb[r0 * P + cb] = sw ? z00 : z01;
+            vb[r1 * P + ca] = sw ? z11 : z10;
+            vb[r1 * P + cb] = sw ? z10 : z11;
         }
     }
 };
@@ -496,12 +511,16 @@ struct OpSuper1 {
     ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr, unsigned = 3u) const {
         const unsigned P = g.P(), lh = g.ls + g.h - 1, vbq = g.vbit[0];
         const unsigned groups = 1u << (2 * lh);
+        const bool sw = dm_swap_cols(vbq, lh, tid);
         for (unsigned t = tid; t < groups; t += nthr) {
             const unsigned r0 = (unsigned)insert0(t >> lh, vbq), c0 = (unsigned)insert0(t & ((1u << lh) - 1), vbq);
             const unsigned r1 = r0 | (1u << vbq), c1 = c0 | (1u << vbq);
-            const unsigned idx[4] = {r0 * P + c0, r0 * P + c1, r1 * P + c0, r1 * P + c1};
-            double2 x[4];
-            for (unsigned m = 0; m < 4; ++m) x[m] = vb[idx[m]];
+            // the column order of each row as in OpMix1 (dm_swap_cols)
+            const unsigned ca = sw ? c1 : c0, cb = sw ? c0 : c1;
+            const double2 y0a = vb[r0 * P + ca], y0b = vb[r0 * P + cb];
+            const double2 y1a = vb[r1 * P + ca], y1b = vb[r1 * P + cb];
+            const double2 x[4] = {sw ? y0b : y0a, sw ? y0a : y0b, sw ? y1b : y1a, sw ? y1a : y1b};
+            double2 out[4];
             for (unsigned m = 0; m < 4; ++m) {
                 double2 acc = c2(0.0, 0.0);
                 for (unsigned j = 0; j < 4; ++j) {          // four FMAs per complex term
@@ -511,33 +530,175 @@ struct OpSuper1 {
                     acc.y = fma(sj.x, x[j].y, acc.y);
                     acc.y = fma(sj.y, x[j].x, acc.y);
                 }
-                vb[idx[m]] = acc;
+                out[m] = acc;
             }
+            vb[r0 * P + ca] = sw ? out[1] : out[0];
+            vb[r0 * P + cb] = sw ? out[0] : out[1];
+            vb[r1 * P + ca] = sw ? out[3] : out[2];
+            vb[r1 * P + cb] = sw ? out[2] : out[3];
         }
     }
 };
 
+// FP64 tensor-core form of the 2-qubit superoperator.  The update of one 4 x 4 group is a real
+// 32 x 32 matrix A (rows: re / im of the 16 outputs; columns: re / im of the 16 inputs) times
+// the group's 32 real inputs; a warp applies it to 8 groups at a time with 4 x 8 steps of
+// mma.sync.m8n8k4.f64 (D = A B + D on 8 x 8 x 4; lane l holds A[l / 4][l % 4], B[l % 4][l / 4]
+// and D[l / 4][2 (l % 4) + i], i = 0, 1).  Row tile mt (0 .. 3) of A holds output
+// o = 8 (mt & 1) + l / 4, real part for mt < 2, imaginary part otherwise; k-step ks (0 .. 7)
+// holds input j = 4 (ks & 3) + l % 4, real part for ks < 4; the columns of B are the 8 groups.
+// One warp instruction does 256 FMA instead of 32, which leaves the issue slots to the loads,
+// stores and index arithmetic around it.
+
+// Staged index of the base element (local row 0, local column 0) of group t: the row and
+// column parts of t with zeros inserted at the gate bits asc[0] < asc[1] (32-bit arithmetic).
+ORKAN_HD unsigned super2_group_base(unsigned P, const unsigned* asc, unsigned lq, unsigned t) {
+    unsigned r = t >> lq, c = t & ((1u << lq) - 1);
+    for (unsigned j = 0; j < 2; ++j) {
+        const unsigned lo = (1u << asc[j]) - 1;
+        r = ((r & ~lo) << 1) | (r & lo);
+        c = ((c & ~lo) << 1) | (c & lo);
+    }
+    return r * P + c;
+}
+
+// A lane's element offsets from a group's base element (the base has zeros at the gate bits,
+// so an element is base + offset): in[r] for its inputs (local row r, local column lane % 4 of
+// group base + lane / 4), out[h] for its outputs (local row 2 h + lane / 16, local column
+// (lane / 4) % 4 of groups base + 2 (lane % 4) + i, i = 0, 1).
+struct Super2Lane {
+    unsigned in[4];
+    unsigned out[2];
+};
+ORKAN_HD Super2Lane super2_lane(const DmGeom& g, unsigned lane) {
+    Super2Lane L;
+    const unsigned P = g.P(), gq = lane >> 2, q = lane & 3u;
+    for (unsigned r = 0; r < 4; ++r) L.in[r] = dm_set_local(0u, r, g.vbit, 2) * P + dm_set_local(0u, q, g.vbit, 2);
+    for (unsigned h = 0; h < 2; ++h)
+        L.out[h] = dm_set_local(0u, 2 * h + (gq >> 2), g.vbit, 2) * P + dm_set_local(0u, gq & 3u, g.vbit, 2);
+    return L;
+}
+
+// Lane's entry of A for row tile mt and k-step ks (superoperator sp, row-major 16 x 16).
+ORKAN_HD double super2_afrag(const double2* sp, unsigned mt, unsigned ks, unsigned lane) {
+    const unsigned o = 8 * (mt & 1) + (lane >> 2), j = 4 * (ks & 3) + (lane & 3);
+    const double2 e = sp[16 * o + j];
+    const bool re_out = mt < 2, re_in = ks < 4;
+    // re out = sum (e.re x.re - e.im x.im), im out = sum (e.im x.re + e.re x.im)
+    return re_out == re_in ? e.x : (re_out ? -e.y : e.y);
+}
+
+#ifdef __CUDACC__
+__device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+        : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+#endif
+
 // 2-qubit superoperator (row-major s[16 * m + j], vec index 4 * row + column of the 4 x 4
 // block over the two gate qubits, local index 2 * bit(q0) + bit(q1)) on 4 x 4 groups.
+// A fragments of one lane (built once per engine block).
+struct Super2Frag {
+    double a[4][8];
+};
+
+// Whether an item of geometry g takes the tensor-core form (8 groups per warp step).  Then
+// the staged block has V >= 16 rows of P = V + 1 slots, at least 272, so it can hold the 256
+// superoperator entries while the fragments are built (dm_op_prepare).
+ORKAN_HD bool super2_mma_form(const DmGeom& g, unsigned nthr) {
+    return g.ls + g.h >= 4 && (nthr & 31u) == 0;
+}
+ORKAN_HD bool super2_stage_fits(const DmGeom& g) { return (unsigned long long)g.V() * g.P() >= 256ull; }
+
 struct OpSuper2 {
     double2 s[256];
-    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr, unsigned = 3u) const {
-#ifdef __CUDA_ARCH__
-        // the superoperator is read 16 times per group: from shared memory (one broadcast
-        // load per complex entry) rather than from the kernel parameters (every thread writes
-        // the same values, and the engine's barriers separate one item's reads from the next
-        // item's writes)
-        __shared__ double2 ss[256];
-        for (unsigned i = tid; i < 256; i += nthr) ss[i] = s[i];
-        __syncthreads();
-        const double2* sp = ss;
-#else
-        const double2* sp = s;
-#endif
+#ifdef __CUDACC__
+    // Tensor-core form of one item with the lane's fragments f: warp w takes groups
+    // 8 w .. 8 w + 7, then 8 (w + warps) ...; the mma of a warp reads every lane's inputs
+    // before any lane stores, and the groups of different warps are disjoint.
+    __device__ void mma_groups(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr, const Super2Frag& f) const {
         const unsigned P = g.P(), lq = g.ls + g.h - 2;
         unsigned asc[2] = {g.vbit[0] < g.vbit[1] ? g.vbit[0] : g.vbit[1],
                            g.vbit[0] < g.vbit[1] ? g.vbit[1] : g.vbit[0]};
         const unsigned groups = 1u << (2 * lq);
+        const unsigned lane = tid & 31u, gq = lane >> 2, q = lane & 3u;
+        const double(&a)[4][8] = f.a;
+        const Super2Lane L = super2_lane(g, lane);
+        {
+            for (unsigned base = 8 * (tid >> 5); base < groups; base += 8 * (nthr >> 5)) {
+                const unsigned ein = super2_group_base(P, asc, lq, base + gq);
+                double b[8];
+#pragma unroll
+                for (unsigned r = 0; r < 4; ++r) {
+                    const double2 x = vb[ein + L.in[r]];
+                    b[r] = x.x;
+                    b[r + 4] = x.y;
+                }
+                double d[4][2];
+#pragma unroll
+                for (unsigned mt = 0; mt < 4; ++mt) {
+                    d[mt][0] = 0.0;
+                    d[mt][1] = 0.0;
+#pragma unroll
+                    for (unsigned ks = 0; ks < 8; ++ks) dmma_884(d[mt][0], d[mt][1], a[mt][ks], b[ks]);
+                }
+#pragma unroll
+                for (unsigned i = 0; i < 2; ++i) {
+                    const unsigned eout = super2_group_base(P, asc, lq, base + 2 * q + i);
+                    vb[eout + L.out[0]] = c2(d[0][i], d[2][i]);
+                    vb[eout + L.out[1]] = c2(d[1][i], d[3][i]);
+                }
+            }
+        }
+    }
+#endif
+
+    // Scalar form (items of fewer than 8 groups), and on the host also the tensor-core form,
+    // carried out by lane 0 of each warp with the fragment layout of the instruction.
+    ORKAN_HD void operator()(const DmGeom& g, double2* vb, unsigned tid, unsigned nthr, unsigned = 3u) const {
+        const double2* sp = s;     // read in the same order by every thread: broadcast loads
+        const unsigned P = g.P(), lq = g.ls + g.h - 2;
+        unsigned asc[2] = {g.vbit[0] < g.vbit[1] ? g.vbit[0] : g.vbit[1],
+                           g.vbit[0] < g.vbit[1] ? g.vbit[1] : g.vbit[0]};
+        const unsigned groups = 1u << (2 * lq);
+#ifndef __CUDA_ARCH__
+        if (super2_mma_form(g, nthr) && super2_stage_fits(g)) {
+            // host: lane 0 of each warp carries out the warp's steps with the fragment layout
+            // of the instruction, through the same index and fragment functions
+            if (tid & 31u) return;
+            for (unsigned base = 8 * (tid >> 5); base < groups; base += 8 * (nthr >> 5)) {
+                double b[32][8], d[32][4][2];
+                for (unsigned l = 0; l < 32; ++l) {
+                    const Super2Lane L = super2_lane(g, l);
+                    const unsigned ein = super2_group_base(P, asc, lq, base + (l >> 2));
+                    for (unsigned r = 0; r < 4; ++r) {
+                        const double2 x = vb[ein + L.in[r]];
+                        b[l][r] = x.x;
+                        b[l][r + 4] = x.y;
+                    }
+                }
+                for (unsigned mt = 0; mt < 4; ++mt) {
+                    double D[8][8] = {};
+                    for (unsigned ks = 0; ks < 8; ++ks)
+                        for (unsigned m = 0; m < 8; ++m)
+                            for (unsigned nn = 0; nn < 8; ++nn)
+                                for (unsigned k = 0; k < 4; ++k)
+                                    D[m][nn] = fma(super2_afrag(sp, mt, ks, 4 * m + k), b[4 * nn + k][ks], D[m][nn]);
+                    for (unsigned l = 0; l < 32; ++l)
+                        for (unsigned i = 0; i < 2; ++i) d[l][mt][i] = D[l >> 2][2 * (l & 3u) + i];
+                }
+                for (unsigned l = 0; l < 32; ++l) {
+                    const Super2Lane L = super2_lane(g, l);
+                    for (unsigned i = 0; i < 2; ++i) {
+                        const unsigned eout = super2_group_base(P, asc, lq, base + 2 * (l & 3u) + i);
+                        vb[eout + L.out[0]] = c2(d[l][0][i], d[l][2][i]);
+                        vb[eout + L.out[1]] = c2(d[l][1][i], d[l][3][i]);
+                    }
+                }
+            }
+            return;
+        }
+#endif
         for (unsigned t = tid; t < groups; t += nthr) {
             const unsigned rb = (unsigned)insert0_sorted(t >> lq, asc, 2);
             const unsigned cb = (unsigned)insert0_sorted(t & ((1u << lq) - 1), asc, 2);
@@ -863,9 +1024,44 @@ __device__ __forceinline__ bool dm_wait_stage(unsigned long long* bar, unsigned 
     return false;
 }
 
+// Per-thread state an op keeps across the items of an engine block: none, except the
+// 2-qubit superoperator's tensor-core fragments, built once per block from the kernel
+// parameters through the staged block (not in use before the first item).
+struct DmNoThreadState {};
+template <class Op> struct DmThreadState { using type = DmNoThreadState; };
+template <> struct DmThreadState<OpSuper2> { using type = Super2Frag; };
+
+template <class Op>
+__device__ __forceinline__ void dm_op_prepare(const Op&, const DmGeom&, DmNoThreadState&, double2*, unsigned,
+                                              unsigned) {}
+template <class Op>
+__device__ __forceinline__ void dm_op_apply(const Op& op, const DmGeom& g, double2* vb, unsigned tid, unsigned nthr,
+                                            unsigned iflags, const DmNoThreadState&) {
+    op(g, vb, tid, nthr, iflags);
+}
+__device__ __forceinline__ void dm_op_prepare(const OpSuper2& op, const DmGeom& g, Super2Frag& f, double2* vb,
+                                              unsigned tid, unsigned nthr) {
+    // the same condition for every block of the launch; only the tensor-core form uses the
+    // fragments, and only then is the staged block large enough to stage the entries
+    if (!super2_mma_form(g, nthr) || !super2_stage_fits(g)) return;
+    for (unsigned i = tid; i < 256; i += nthr) vb[i] = op.s[i];
+    __syncthreads();
+#pragma unroll
+    for (unsigned mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (unsigned ks = 0; ks < 8; ++ks) f.a[mt][ks] = super2_afrag(vb, mt, ks, tid & 31u);
+    __syncthreads();                                   // read before the first item's copies land
+}
+__device__ __forceinline__ void dm_op_apply(const OpSuper2& op, const DmGeom& g, double2* vb, unsigned tid,
+                                            unsigned nthr, unsigned iflags, const Super2Frag& f) {
+    if (super2_mma_form(g, nthr) && super2_stage_fits(g)) op.mma_groups(g, vb, tid, nthr, f);
+    else op(g, vb, tid, nthr, iflags);
+}
+
 // Blocks per SM the register budget is held to: three blocks with a 64 x 64 staged block
 // fill the shared memory, and the bulk copies of one overlap the compute of the others.
-// The 2-qubit superoperator holds a whole 4 x 4 group in registers and gets two.
+// The 2-qubit superoperator keeps 32 tensor-core fragment values per lane across the items
+// (64 registers) and gets two.
 template <class Op> struct DmMinBlocks { static constexpr int value = 3; };
 template <> struct DmMinBlocks<OpSuper2> { static constexpr int value = 2; };
 
@@ -885,6 +1081,8 @@ __global__ void __launch_bounds__(kDmBlock, DmMinBlocks<Op>::value) k_dm_engine(
         mbar_init(bar, 1);
         fence_mbar_init();
     }
+    typename DmThreadState<Op>::type ts;
+    dm_op_prepare(op, g, ts, vb, tid, nthr);
     unsigned parity = 0;
     bool ok = true;
     for (idx_t w = blockIdx.x; w < g.items; w += gridDim.x) {
@@ -914,7 +1112,7 @@ __global__ void __launch_bounds__(kDmBlock, DmMinBlocks<Op>::value) k_dm_engine(
             dm_fixups<Map>(g, pd, vb, 0, fix0, tid, nthr);
             __syncthreads();
         }
-        op(g, vb, tid, nthr, iflags & 3u);
+        dm_op_apply(op, g, vb, tid, nthr, iflags & 3u, ts);
         __syncthreads();
         if (fix1) {
             dm_fixups<Map>(g, pd, vb, 1, fix1, tid, nthr);

@@ -289,6 +289,20 @@ int emu_dm_superop2(int layout, unsigned log_tile, double* rho, uint64_t len, un
     return engine_dispatch(layout, log_tile, rho, len, n, g, op, reads, writes, oob);
 }
 
+// Geometry of channel_2q on (q0, q1): -1 when there is none, else bit 0 set when the items
+// take the tensor-core form and bit 1 when the staged block holds the 256 superoperator
+// entries that the engine stages there before the first item (the device code stages only
+// when both hold); out = {V, P, dynamic shared-memory bytes of an engine block}.
+int emu_super2_geometry(int layout, unsigned log_tile, unsigned n, unsigned q0, unsigned q1, uint64_t* out) {
+    DmGeom g;
+    const unsigned q[2] = {q0, q1};
+    if (!dm_geometry(n, 2, q, ls_max_for(layout, log_tile), &g, emu_max_v())) return -1;
+    out[0] = g.V();
+    out[1] = g.P();
+    out[2] = dm_block_smem_bytes(g);
+    return (super2_mma_form(g, kDmBlock) ? 1 : 0) | (super2_stage_fits(g) ? 2 : 0);
+}
+
 int emu_dm_phase(int layout, unsigned log_tile, double* rho, uint64_t len, unsigned n, unsigned k,
                  const unsigned* qubits, const double* phase, uint32_t* reads, uint32_t* writes, uint64_t* oob) {
     EmuMem mem{reinterpret_cast<double2*>(rho), len, reads, writes, oob};

@@ -165,6 +165,31 @@ def test_superop2_oracle_is_the_kraus_sum():
         assert np.abs(R.apply_superop2(rho, sop, q0, q1) - want).max() < 1e-13
 
 
+@pytest.mark.parametrize("max_v", ["8", "16", "32", "64"])
+def test_superop2_fragment_staging_stays_in_the_block(max_v, monkeypatch):
+    """Before its first item an engine block running channel_2q in the tensor-core form stages
+    the 256 superoperator entries in its staged block: for every geometry of 2..14 qubits,
+    both layouts and tile sizes and every block-side cap, the items that take that form have
+    a staged block of at least 256 slots inside the block's dynamic shared memory."""
+    import ctypes as C
+    monkeypatch.setenv("ORKAN_DM_MAX_V", max_v)
+    f = kemu.lib().emu_super2_geometry
+    f.argtypes = [C.c_int, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.POINTER(C.c_uint64)]
+    out = (C.c_uint64 * 3)()
+    seen = set()
+    for kind, lt in LAYOUTS:
+        for n in range(2, 15):
+            for q0, q1 in itertools.permutations(range(n), 2):
+                r = f(kemu.LAYOUT[kind], lt, n, q0, q1, out)
+                assert r >= 0, (kind, lt, n, q0, q1)
+                V, P, smem = out[0], out[1], out[2]
+                seen.add((r & 1, V))
+                if r & 1:
+                    assert r & 2 and V >= 16 and V * P >= 256, (kind, lt, n, q0, q1, V, P)
+                    assert smem >= 16 + V * P * 16
+    assert any(m for m, _ in seen) and any(not m for m, _ in seen)
+
+
 @pytest.mark.parametrize("kind,lt", LAYOUTS)
 @pytest.mark.parametrize("n", [2, 3, 5, 7])
 def test_dm_superop2_emulated(kind, lt, n):
