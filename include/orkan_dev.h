@@ -44,6 +44,15 @@ unsigned orkan_get_gate_fusion(void);
 int orkan_state_upload(state_t *state, const cplx_t *host);
 int orkan_state_download(const state_t *state, cplx_t *host);
 
+/* Asynchronous upload: enqueues the copy of host into the state's storage on stream (a
+ * cudaStream_t; NULL: the library stream) and returns without waiting.  The copy starts after
+ * all work enqueued so far on the library stream (queued gates are launched first), so work
+ * that still reads or writes the state finishes before it is overwritten.  The caller keeps
+ * host valid and unchanged until the copy has completed (pinned memory for a copy that
+ * overlaps kernels), and orders later library work on the state after it, e.g. by making
+ * the library stream wait for an event recorded on stream.  Returns 0 or a cudaError_t. */
+int orkan_state_upload_async(state_t *state, const cplx_t *host, void *stream);
+
 /* 2-qubit channel on a density matrix: sop from kraus_to_superop of 2-qubit Kraus operators
  * (16 x 16), local index 2 * bit(q0) + bit(q1).  The reference's channel_1q takes 1-local
  * superoperators only; this is its 2-local counterpart, with the same validation behaviour

@@ -111,6 +111,8 @@ class Orkan:
         L.orkan_get_stream.restype = vp
         L.orkan_state_upload.argtypes = [P, vp]
         L.orkan_state_upload.restype = C.c_int
+        L.orkan_state_upload_async.argtypes = [P, vp, vp]
+        L.orkan_state_upload_async.restype = C.c_int
         L.orkan_state_download.argtypes = [P, vp]
         L.orkan_state_download.restype = C.c_int
         L.orkan_launch_count.restype = C.c_ulonglong
@@ -146,6 +148,14 @@ class Orkan:
         if arr.size != self.lib.state_len(C.byref(s)):
             raise OrkanError("storage length does not match the state")
         rc = self.lib.orkan_state_upload(C.byref(s), arr.ctypes.data)
+        if rc:
+            raise OrkanError(f"upload failed: CUDA error {rc}")
+
+    def upload_async(self, s: StateT, host_ptr: int, stream: int | None = None) -> None:
+        """orkan_state_upload_async: the copy of state_len(s) elements from host_ptr is enqueued
+        on stream (a cudaStream_t handle; None: the library stream) after the library stream's
+        pending work; the caller keeps the host buffer alive and orders later work after it."""
+        rc = self.lib.orkan_state_upload_async(C.byref(s), C.c_void_p(host_ptr), C.c_void_p(stream))
         if rc:
             raise OrkanError(f"upload failed: CUDA error {rc}")
 

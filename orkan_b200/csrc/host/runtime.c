@@ -217,6 +217,25 @@ int orkan_state_upload(state_t *state, const cplx_t *host) {
     return (int)e;
 }
 
+int orkan_state_upload_async(state_t *state, const cplx_t *host, void *stream) {
+    if (!state || !state->data || !host) return (int)cudaErrorInvalidValue;
+    orkan_flush();
+    const size_t bytes = (size_t)state_len(state) * sizeof(cplx_t);
+    cudaStream_t st = stream ? (cudaStream_t)stream : (cudaStream_t)g_stream;
+    cudaError_t e = cudaSuccess;
+    if (st != (cudaStream_t)g_stream) {
+        /* the copy waits for the library stream's work enqueued so far */
+        cudaEvent_t ev;
+        e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return (int)e;
+        e = cudaEventRecord(ev, (cudaStream_t)g_stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ev, 0);
+        cudaEventDestroy(ev);
+        if (e != cudaSuccess) return (int)e;
+    }
+    return (int)cudaMemcpyAsync(state->data, host, bytes, cudaMemcpyHostToDevice, st);
+}
+
 int orkan_state_download(const state_t *state, cplx_t *host) {
     if (!state || !state->data || !host) return (int)cudaErrorInvalidValue;
     orkan_flush();
