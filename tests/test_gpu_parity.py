@@ -152,6 +152,26 @@ def test_channel_2q(request, lt, kind):
 
 
 @pytest.mark.parametrize("lt", [3, 5])
+@pytest.mark.parametrize("kind", ["packed", "tiled"])
+def test_channel_2q_10q(request, lt, kind):
+    """2-qubit channels at 10 qubits, where every engine geometry takes the FP64 tensor-core
+    form (both qubits inside a sub-tile, one or both above it, adjacent and spread, either
+    order), against the oracle's restatement."""
+    ork = lib_for(request, lt)
+    rng = np.random.default_rng(21)
+    n = 10
+    rho = rand_rho(n, 321)
+    st = ork.state(kind, n, R.to_storage(kind, rho, lt))
+    iso, _ = np.linalg.qr(rng.standard_normal((16, 4)) + 1j * rng.standard_normal((16, 4)))
+    sop = ork.superop([iso[4 * i:4 * i + 4, :] for i in range(4)])
+    for q0, q1 in ((0, 1), (1, 0), (0, 9), (9, 0), (2, 7), (5, 6), (8, 9), (9, 4), (3, 4)):
+        ork.channel_2q(st, sop, q0, q1)
+        rho = R.apply_superop2(rho, sop, q0, q1)
+    assert np.abs(ork.storage(st) - R.to_storage(kind, rho, lt)).max() <= TOL
+    ork.free(st)
+
+
+@pytest.mark.parametrize("lt", [3, 5])
 @pytest.mark.parametrize("kind", ["pure", "packed", "tiled"])
 def test_mean_exp_diag(request, lt, kind):
     ork = lib_for(request, lt)
