@@ -13,6 +13,8 @@ capture of the same command can be set against them.  Cases (the sweep's kernel 
   tiled_phase / packed_phase     T on 0, 7, n-1;  tiled_exp_diag / packed_exp_diag
   tiled_channel_2q / packed_channel_2q   random 2-qubit channel on (0, n-1), (5, 6)
   pure_fused      a 48-gate random circuit, fused
+  pure_fused_costs   crafted runs (1-48 gates, 1-8 register stages), each queued and flushed
+                  as one fused launch, timed with CUDA events (prints ms per launch)
 The states are larger than L2 at the default sizes (2 GiB statevector, 0.5 GB density
 matrices), so DRAM figures are meaningful, and small enough for a short capture.
 """
@@ -42,7 +44,7 @@ def main(argv=None) -> int:
     kind = case.split("_")[0]
     n = args.pure_qubits if kind == "pure" else args.mixed_qubits
     h = n // 2
-    ork.set_gate_fusion(48 if case == "pure_fused" else 0)
+    ork.set_gate_fusion(48 if case.startswith("pure_fused") else 0)
     st = ork.state(kind, n)
     W.fill_state_on_device(ork, st, kind, n, seed=1, log_tile=5)
     ops = []                                           # (callable, algorithmic bytes)
@@ -80,6 +82,36 @@ def main(argv=None) -> int:
                 ork.gate(st, g, qs, th)
             ork.flush()
         ops.append((run, alg))
+    elif case == "pure_fused_costs":
+        runs = [("1 H on qubit 0", [("h", (0,), None)]),
+                ("8 H on qubits 0-2", [("h", (q % 3,), None) for q in range(8)]),
+                ("24 H on qubits 0-2", [("h", (q % 3,), None) for q in range(24)]),
+                ("48 H on qubits 0-2", [("h", (q % 3,), None) for q in range(48)]),
+                ("24 Rx on qubits 0-2", [("rx", (q % 3,), 0.3) for q in range(24)]),
+                ("24 T on qubits 0-2", [("t", (q % 3,), None) for q in range(24)]),
+                ("24 CX within qubits 0-2", [("cx", (q % 3, (q + 1) % 3), None) for q in range(24)]),
+                (f"24 CX, control qubit {n - 1}, targets 0-2", [("cx", (n - 1, q % 3), None) for q in range(24)]),
+                ("6 H on qubits 0-5", [("h", (q,), None) for q in range(6)]),
+                ("9 H on qubits 0-8", [("h", (q,), None) for q in range(9)]),
+                ("11 H on qubits 0-10", [("h", (q,), None) for q in range(11)]),
+                ("24 H cycling over qubits 0-8", [("h", (q % 9,), None) for q in range(24)])]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for label, circ in runs:
+            def run(circ=circ):
+                for g, qs, th in circ:
+                    ork.gate(st, g, qs, th)
+                ork.flush()
+            for _ in range(2):
+                run()
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(10 * args.reps):
+                run()
+            e1.record()
+            torch.cuda.synchronize()
+            print(f"{label}: {e0.elapsed_time(e1) / (10 * args.reps):.3f} ms per launch")
+        ork.free(st)
+        return 0
     else:
         print(f"unknown case {case}", file=sys.stderr)
         return 2
