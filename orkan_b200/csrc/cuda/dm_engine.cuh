@@ -595,8 +595,6 @@ __device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, doubl
 }
 #endif
 
-// 2-qubit superoperator (row-major s[16 * m + j], vec index 4 * row + column of the 4 x 4
-// block over the two gate qubits, local index 2 * bit(q0) + bit(q1)) on 4 x 4 groups.
 // A fragments of one lane (built once per engine block).
 struct Super2Frag {
     double a[4][8];
@@ -610,6 +608,8 @@ ORKAN_HD bool super2_mma_form(const DmGeom& g, unsigned nthr) {
 }
 ORKAN_HD bool super2_stage_fits(const DmGeom& g) { return (unsigned long long)g.V() * g.P() >= 256ull; }
 
+// 2-qubit superoperator (row-major s[16 * m + j], vec index 4 * row + column of the 4 x 4
+// block over the two gate qubits, local index 2 * bit(q0) + bit(q1)) on 4 x 4 groups.
 struct OpSuper2 {
     double2 s[256];
 #ifdef __CUDACC__
@@ -624,30 +624,28 @@ struct OpSuper2 {
         const unsigned lane = tid & 31u, gq = lane >> 2, q = lane & 3u;
         const double(&a)[4][8] = f.a;
         const Super2Lane L = super2_lane(g, lane);
-        {
-            for (unsigned base = 8 * (tid >> 5); base < groups; base += 8 * (nthr >> 5)) {
-                const unsigned ein = super2_group_base(P, asc, lq, base + gq);
-                double b[8];
+        for (unsigned base = 8 * (tid >> 5); base < groups; base += 8 * (nthr >> 5)) {
+            const unsigned ein = super2_group_base(P, asc, lq, base + gq);
+            double b[8];
 #pragma unroll
-                for (unsigned r = 0; r < 4; ++r) {
-                    const double2 x = vb[ein + L.in[r]];
-                    b[r] = x.x;
-                    b[r + 4] = x.y;
-                }
-                double d[4][2];
+            for (unsigned r = 0; r < 4; ++r) {
+                const double2 x = vb[ein + L.in[r]];
+                b[r] = x.x;
+                b[r + 4] = x.y;
+            }
+            double d[4][2];
 #pragma unroll
-                for (unsigned mt = 0; mt < 4; ++mt) {
-                    d[mt][0] = 0.0;
-                    d[mt][1] = 0.0;
+            for (unsigned mt = 0; mt < 4; ++mt) {
+                d[mt][0] = 0.0;
+                d[mt][1] = 0.0;
 #pragma unroll
-                    for (unsigned ks = 0; ks < 8; ++ks) dmma_884(d[mt][0], d[mt][1], a[mt][ks], b[ks]);
-                }
+                for (unsigned ks = 0; ks < 8; ++ks) dmma_884(d[mt][0], d[mt][1], a[mt][ks], b[ks]);
+            }
 #pragma unroll
-                for (unsigned i = 0; i < 2; ++i) {
-                    const unsigned eout = super2_group_base(P, asc, lq, base + 2 * q + i);
-                    vb[eout + L.out[0]] = c2(d[0][i], d[2][i]);
-                    vb[eout + L.out[1]] = c2(d[1][i], d[3][i]);
-                }
+            for (unsigned i = 0; i < 2; ++i) {
+                const unsigned eout = super2_group_base(P, asc, lq, base + 2 * q + i);
+                vb[eout + L.out[0]] = c2(d[0][i], d[2][i]);
+                vb[eout + L.out[1]] = c2(d[1][i], d[3][i]);
             }
         }
     }
