@@ -503,35 +503,49 @@ def plain_qaoa_mean(lib, n, cost, g, b):
 
 
 def batched_cpu_baseline(ns, edges, g, b, budget_s):
-    """The reference library's per-call path on the host cores, timed on the smallest
-    instances of the batch; the whole batch's time is projected from the measured seconds
-    per amplitude-gate (each instance costs p (n + 1) + 2 calls over 2^n amplitudes)."""
-    import numpy as np
+    """The reference library's per-call path on the host cores, timed on instances of every
+    qubit count of the batch: round robin over the counts, smallest first, one instance of
+    each count per round, the first round whole and at most two more while the budget lasts.
+    The whole batch's time is the sum over qubit counts of (instances of that count) x
+    (measured seconds per instance of that count)."""
     from oracle import restate as R
     cores = host_cores()
     lib = reference_lib(cores)
     if lib is None:
         return None
-    p = g.shape[1]
-    work = lambda n: (p * (n + 1) + 2) * float(2 ** n)
-    order = np.argsort(ns, kind="stable")
-    done, secs, units = 0, 0.0, 0.0
-    for i in order:
-        if secs > budget_s:
+    by_n = {}
+    for i, n in enumerate(ns):
+        by_n.setdefault(int(n), []).append(i)
+    counts = sorted(by_n)
+    t_sum = {n: 0.0 for n in counts}
+    done = {n: 0 for n in counts}
+    secs, rnd = 0.0, 0
+    while True:
+        progressed = False
+        for n in counts:
+            if rnd > 0 and secs > budget_s:
+                break
+            if rnd >= len(by_n[n]):
+                continue
+            i = by_n[n][rnd]
+            cost = R.maxcut_cost(n, edges[i])
+            t0 = time.perf_counter()
+            plain_qaoa_mean(lib, n, cost, g[i], b[i])
+            dt = time.perf_counter() - t0
+            t_sum[n] += dt
+            done[n] += 1
+            secs += dt
+            progressed = True
+        rnd += 1
+        if secs > budget_s or not progressed or rnd >= 3:
             break
-        n = int(ns[i])
-        cost = R.maxcut_cost(n, edges[i])
-        t0 = time.perf_counter()
-        plain_qaoa_mean(lib, n, cost, g[i], b[i])
-        secs += time.perf_counter() - t0
-        units += work(n)
-        done += 1
-    total = sum(work(int(n)) for n in ns)
-    projected = secs / units * total
+    projected = sum(len(by_n[n]) * t_sum[n] / done[n] for n in counts)
+    per_n = ", ".join(f"{n} q: {done[n]}" for n in counts)
     return {"value": len(ns) / projected, "unit": "evals/s", "cores": cores, "kind": "reference",
-            "sample": f"{done} instances of {int(ns[order[0]])}..{int(ns[order[done - 1]])} qubits through the "
-                      f"reference's per-call API ({secs:.1f} s), projected to the {len(ns)}-instance batch by "
-                      f"amplitude-calls, OpenMP threads = {cores}"}
+            "seconds_per_instance": {str(n): t_sum[n] / done[n] for n in counts},
+            "sample": f"{sum(done.values())} instances of every qubit count of the batch ({per_n}) through the "
+                      f"reference's per-call API ({secs:.1f} s); the {len(ns)}-instance batch's time is the sum "
+                      f"over qubit counts of instances x measured seconds per instance, OpenMP threads = {cores}"}
 
 
 def batched_leg(args, ork, clocks_cls, local, dist=None, rank=0, world=1):

@@ -407,7 +407,14 @@ def plus_state(kind: str, n: int) -> np.ndarray:
 # QAOA-style circuits as compositions of reference calls (the batched entry point's checker)
 # ----------------------------------------------------------------------------------------
 def maxcut_cost(n: int, edges, weights=None) -> np.ndarray:
-    """cost[x] = sum_e w_e [bit u_e of x != bit v_e of x], summed in edge order."""
+    """cost[x] = sum_e w_e [bit u_e of x != bit v_e of x], summed in edge order (unit
+    weights: counted in small integers, the same values)."""
+    if weights is None:
+        x = np.arange(1 << n, dtype=np.uint32)
+        cnt = np.zeros(1 << n, dtype=np.uint8 if len(edges) < 256 else np.uint32)
+        for u, v in edges:
+            np.add(cnt, ((x >> u) ^ (x >> v)) & 1, out=cnt, casting="unsafe")
+        return cnt.astype(np.float64)
     x = np.arange(1 << n, dtype=np.int64)
     cost = np.zeros(1 << n, dtype=np.float64)
     for e, (u, v) in enumerate(edges):
