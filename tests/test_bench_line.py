@@ -6,6 +6,7 @@ import json
 import os
 
 import bench
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -42,3 +43,24 @@ def test_learned_legs_run_at_their_configured_sizes(monkeypatch):
     a = bench.parse_args()
     assert a.surrogate_pairs == 65536 and a.noisy_pairs > 0
     assert a.batch_instances == 4096 and a.batch_check == -1 and a.circuit_gates == 200
+
+
+def test_batched_cpu_baseline_times_every_qubit_count():
+    """The batched leg's CPU baseline times the reference library on instances of every qubit
+    count of the batch and weights each count's seconds per instance by its instances."""
+    import numpy as np
+    from oracle import ref
+    if not ref.available(5):
+        pytest.skip("the reference library (oracle/_ref) is not built")
+    from orkan_b200.batch import random_regular_graph
+    rng = np.random.default_rng(3)
+    ns = np.array([4, 6, 4, 8, 6, 4, 8, 8])
+    edges = [random_regular_graph(int(n), 3, rng) for n in ns]
+    g = rng.uniform(0, np.pi, (len(ns), 2))
+    b = rng.uniform(0, np.pi / 2, (len(ns), 2))
+    out = bench.batched_cpu_baseline(ns, edges, g, b, 0.0)
+    per = out["seconds_per_instance"]
+    assert sorted(per) == ["4", "6", "8"]
+    want = sum(int(np.sum(ns == n)) * per[str(n)] for n in (4, 6, 8))
+    assert out["value"] == pytest.approx(len(ns) / want)
+    assert "every qubit count" in out["sample"]
