@@ -180,19 +180,28 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "kernel_classes_dram_27q_13q.md")
+
+
 def profiled_traffic():
-    """ncu DRAM traffic of each kernel class from the committed summary: {class: (dram bytes
-    of the captured launch, algorithmic bytes of that launch)}."""
-    path = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
-    try:
-        with open(path) as f:
-            raw = json.load(f)
-    except Exception:
-        return {}
+    """ncu DRAM traffic of each kernel class from the committed summary's table: {class:
+    (DRAM bytes per captured launch, algorithmic bytes of that launch)}.  Table rows are
+    `| <class> (<gates>) | <kernel> | <launches> | <algorithmic MB> | <DRAM MB> | <ratio> |`."""
     out = {}
-    for c, v in raw.items():
-        if isinstance(v, dict) and v.get("dram_bytes") and v.get("algorithmic_bytes"):
-            out[c] = (float(v["dram_bytes"]), float(v["algorithmic_bytes"]))
+    try:
+        with open(PROFILE_TRAFFIC) as f:
+            lines = f.readlines()
+    except OSError:
+        return out
+    for line in lines:
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(cells) != 6 or not cells[0] or cells[0].startswith(("case", "---")):
+            continue
+        try:
+            alg, dram = float(cells[3]) * 1e6, float(cells[4]) * 1e6
+        except ValueError:
+            continue
+        out[cells[0].split()[0]] = (dram, alg)
     return out
 
 
