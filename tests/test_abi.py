@@ -164,3 +164,29 @@ def test_batch_entry_points_declared_and_validate_without_gpu():
     assert create([4], [2, 2], [0, 1]) == (1, None)         # self loop
     assert create([4], [0, 1], [0, 1], p=0) == (1, None)    # no layers
     assert create([4, 4], [0, 1], [0, 1, 0]) == (1, None)   # decreasing offsets
+
+
+def test_state_upload_entry_points_validate_without_gpu():
+    """orkan_dev.h: the synchronous and asynchronous uploads and the download reject a null
+    state, a state without storage and a null host buffer (cudaErrorInvalidValue = 1) before
+    touching a device."""
+    from orkan_b200.build import library_path
+    decl = declared_functions()
+    for f in ("orkan_state_upload", "orkan_state_upload_async", "orkan_state_download"):
+        assert f in decl
+    lib = C.CDLL(library_path(5))
+
+    class StateT(C.Structure):
+        _fields_ = [("type", C.c_int), ("data", C.c_void_p), ("qubits", C.c_ubyte)]
+
+    buf = (C.c_double * 8)()
+    empty = StateT(0, None, 1)
+    lib.orkan_state_upload_async.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.orkan_state_upload.argtypes = [C.c_void_p, C.c_void_p]
+    lib.orkan_state_download.argtypes = [C.c_void_p, C.c_void_p]
+    assert lib.orkan_state_upload_async(None, buf, None) == 1
+    assert lib.orkan_state_upload_async(C.byref(empty), buf, None) == 1
+    assert lib.orkan_state_upload(C.byref(empty), buf) == 1
+    assert lib.orkan_state_download(C.byref(empty), buf) == 1
+    fake = StateT(0, C.c_void_p(0x1000), 1)
+    assert lib.orkan_state_upload_async(C.byref(fake), None, None) == 1
