@@ -32,6 +32,29 @@ __global__ void k_qaoa_cost(CostT* cost, unsigned n, const unsigned char* edges,
     }
 }
 
+// Transposed byte costs for the high passes of chunks of 2^C: dst[col 2^R + row] =
+// src[row 2^C + col] with R = n - C (qaoa_cost_t_index), through 32 x 32 tiles in shared
+// memory so that reads and writes are both runs of consecutive bytes.
+__global__ void k_qaoa_cost_transpose(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, unsigned n,
+                                      unsigned C) {
+    __shared__ uint8_t tile[32][33];
+    const idx_t rows = idx_t(1) << (n - C), cols = idx_t(1) << C;
+    const idx_t tiles_c = (cols + 31) / 32, tiles = ((rows + 31) / 32) * tiles_c;
+    for (idx_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const idx_t r0 = (t / tiles_c) * 32, c0 = (t % tiles_c) * 32;
+        for (unsigned i = threadIdx.y; i < 32; i += blockDim.y) {
+            const idx_t r = r0 + i, c = c0 + threadIdx.x;
+            if (r < rows && c < cols) tile[i][threadIdx.x] = src[r * cols + c];
+        }
+        __syncthreads();
+        for (unsigned i = threadIdx.y; i < 32; i += blockDim.y) {
+            const idx_t c = c0 + i, r = r0 + threadIdx.x;
+            if (r < rows && c < cols) dst[c * rows + r] = tile[threadIdx.x][i];
+        }
+        __syncthreads();
+    }
+}
+
 // table[(pos p + k) tstride + c] = (cos, sin)(c * gamma[pos p + k]) for c <= cmax of pos
 __global__ void k_qaoa_tables(const unsigned* cmax, const double* gamma, unsigned count, unsigned p,
                               unsigned tstride, double2* table) {
@@ -174,6 +197,8 @@ struct Graph {                     // one distinct cost function
     std::vector<double> w;
     unsigned cmax;                 // byte costs: integer maximum; else 0xffffffff
     void* d_cost = nullptr;
+    uint8_t* d_cost_t = nullptr;   // byte costs: transposed for high passes of chunks of 2^cost_t_C
+    unsigned cost_t_C = 0;         // 0: not filled yet
 };
 
 struct Launch {
@@ -295,7 +320,8 @@ Plan make_plan(const orkan_qaoa* b, const std::vector<unsigned>& sel) {
                     for (size_t k : grp) {
                         QaoaInst r;
                         r.psi = reinterpret_cast<double2*>(off[k - first]);
-                        r.cost = b->graphs[b->gid[sel[k]]].d_cost;
+                        const Graph& gr = b->graphs[b->gid[sel[k]]];
+                        r.cost = (L.kind == kQaoaHigh && bytes_cost) ? static_cast<const void*>(gr.d_cost_t) : gr.d_cost;
                         r.item0 = acc;
                         r.n = nq;
                         r.pos = sel[k];
@@ -321,9 +347,25 @@ Plan make_plan(const orkan_qaoa* b, const std::vector<unsigned>& sel) {
     return pl;
 }
 
-// Device side of a plan: arena, partial sums and the instance records.
+// Device side of a plan: arena, partial sums, the instance records, and the transposed byte
+// costs of the plan's high passes for their chunk size.
 int upload_plan(orkan_qaoa* b, Plan& pl) {
     int rc;
+    bool transposed = false;
+    for (const auto& L : pl.launches) {
+        if (L.what != 0 || L.kind != kQaoaHigh || !L.bytes) continue;
+        for (unsigned k = L.inst_off; k < L.inst_off + L.ninst; ++k) {
+            Graph& g = b->graphs[b->gid[pl.inst[k].pos]];
+            if (g.cost_t_C == L.C) continue;
+            const idx_t tiles = ((idx_t(1) << (g.n - L.C)) + 31) / 32 * (((idx_t(1) << L.C) + 31) / 32);
+            const unsigned grid = (unsigned)std::min<idx_t>(tiles, (idx_t)sm_count() * 8);
+            k_qaoa_cost_transpose<<<grid, dim3(32, 8), 0, b->cap>>>(g.d_cost_t, (const uint8_t*)g.d_cost, g.n, L.C);
+            if ((rc = (int)cudaGetLastError())) return rc;
+            g.cost_t_C = L.C;
+            transposed = true;
+        }
+    }
+    if (transposed && (rc = (int)cudaStreamSynchronize(b->cap))) return rc;
     if (pl.arena > b->arena_bytes) {
         cudaFree(b->d_arena);
         b->d_arena = nullptr;
@@ -517,8 +559,9 @@ int orkan_qaoa_create(orkan_qaoa_t** out, unsigned count, const unsigned* n_qubi
         const idx_t dim = idx_t(1) << g.n;
         unsigned char* d_e = nullptr;
         double* d_w = nullptr;
-        const size_t cbytes = bytes ? ((dim + 15) / 16) * 16 : dim * 8;     // byte costs: whole 4-byte words
-        if ((rc = (int)cudaMalloc(&g.d_cost, cbytes)) || (rc = dalloc(&d_e, g.edges.size())) ||
+        const size_t cbytes = bytes ? ((dim + 15) / 16) * 16 : dim * 8;     // byte costs: whole 16-byte units
+        if ((rc = (int)cudaMalloc(&g.d_cost, cbytes)) ||
+            (bytes && (rc = (int)cudaMalloc(&g.d_cost_t, cbytes))) || (rc = dalloc(&d_e, g.edges.size())) ||
             (rc = dalloc(&d_w, g.w.size()))) {
             cudaFree(d_e);
             orkan_qaoa_destroy(b);
@@ -739,7 +782,10 @@ void orkan_qaoa_destroy(orkan_qaoa_t* b) {
     if (!b) return;
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->cap) cudaStreamDestroy(b->cap);
-    for (auto& g : b->graphs) cudaFree(g.d_cost);
+    for (auto& g : b->graphs) {
+        cudaFree(g.d_cost);
+        cudaFree(g.d_cost_t);
+    }
     cudaFree(b->d_cmax);
     cudaFree(b->d_gamma);
     cudaFree(b->d_rx);

@@ -53,7 +53,8 @@ enum QaoaKind : unsigned { kQaoaFull = 0, kQaoaLow = 1, kQaoaHigh = 2 };
 
 struct QaoaInst {
     double2* psi;          // 2^n amplitudes (unused by full passes)
-    const void* cost;      // 2^n costs: double, or uint8_t (byte costs)
+    const void* cost;      // 2^n costs: double, or uint8_t (byte costs; in high passes the
+                           // transposed array of qaoa_cost_t_index)
     idx_t item0;           // first work item of this instance in the pass
     unsigned n;
     unsigned pos;          // row of the instance in the angle arrays and tables
@@ -285,7 +286,7 @@ ORKAN_HD double2 qaoa_phase(CostT c, double gamma, const double2* table) {
 
 // Shared memory of one block: kQaoaRing buffers, each vb[2^C] amplitudes (padded), the
 // phase table (byte costs) and the costs: FP64 costs one per padded slot (cw), byte costs
-// as a byte array cb copied in runs of 4-16 bytes (see qaoa_cost_index); then red[nthr + 32].
+// as a byte array cb copied in 16-byte runs (see qaoa_cost_index); then red[nthr + 32].
 constexpr unsigned kQaoaRing = 2;
 
 template <class CostT>
@@ -297,24 +298,28 @@ struct QaoaSmem {
     double* red;
 };
 
-// Position of slot s's byte cost in cb.  Low and full chunks: s (the chunk's costs are
-// contiguous; chunks of fewer than 4 amplitudes copy the aligned 4-byte word holding them,
-// so their costs start at byte (chunk 2^C) mod 4).  High chunks (s = row + col 2^R): a row's W = 2^lw costs are contiguous in
-// memory, so each row's run is copied whole: cb[row W + col] when W >= 4; for W < 4 the
-// row's 4-byte aligned word is copied to cb[4 row .. 4 row + 3] and the cost sits at byte
-// (c W + col) mod 4 of it (c: the chunk index).
-ORKAN_HD unsigned qaoa_cost_index(unsigned kind, unsigned C, unsigned R, unsigned lw, idx_t chunk, unsigned s) {
-    if (kind == kQaoaFull) return s;
-    if (kind == kQaoaLow) return C >= 2 ? s : (unsigned)((chunk << C) & 3u) + s;
-    const unsigned row = s & ((1u << R) - 1), col = s >> R;
-    if (lw >= 2) return (row << lw) + col;
-    return 4u * row + (unsigned)(((chunk << lw) + col) & 3u);
+// Byte costs of high passes come from the instance's transposed cost array,
+// cost_t[col 2^R + row] = cost[row 2^C + col] (R = n - C), so that a high chunk's costs, the
+// W columns chunk W .. chunk W + W - 1 of every row in slot order (s = row + col 2^R), are
+// the contiguous run cost_t[chunk 2^C .. chunk 2^C + 2^C) and copy in 16-byte pieces like a
+// low chunk's (instead of a 1-4 byte word from each of 2^R rows 2^C bytes apart).
+ORKAN_HD idx_t qaoa_cost_t_index(unsigned n, unsigned C, idx_t x) {
+    const unsigned R = n - C;
+    return ((x & ((idx_t(1) << C) - 1)) << R) | (x >> C);
 }
 
-// Bytes of the byte-cost array of a chunk of 2^C amplitudes: 4 per slot covers high chunks
-// with W < 4 (4 bytes per row, at most 2^C rows), at least 16 for the 16-byte copies of
-// tiny full chunks.
-ORKAN_HD size_t qaoa_cost_bytes(unsigned C) { return C < 2 ? 16u : (size_t(4) << C); }
+// Position of slot s's byte cost in cb: s, the chunk's costs being contiguous (low and full
+// chunks in the cost array, high chunks in the transposed one); chunks of fewer than 4
+// costs copy the aligned 4-byte word holding them, so their costs start at byte
+// (chunk 2^C) mod 4.
+ORKAN_HD unsigned qaoa_cost_index(unsigned kind, unsigned C, idx_t chunk, unsigned s) {
+    if (kind == kQaoaFull) return s;
+    return C >= 2 ? s : (unsigned)((chunk << C) & 3u) + s;
+}
+
+// Bytes of the byte-cost array of a chunk of 2^C amplitudes, at least 16 for the 16-byte
+// copies of tiny full chunks.
+ORKAN_HD size_t qaoa_cost_bytes(unsigned C) { return C < 4 ? 16u : (size_t(1) << C); }
 
 // Phase-table entries a buffer holds: kQaoaMaxTable for byte costs, none for FP64 costs.
 template <class CostT>
@@ -362,8 +367,8 @@ ORKAN_HD QaoaSmem<CostT> qaoa_smem_at(unsigned char* base, unsigned C, unsigned 
 
 // Fill of one work item's buffer: asynchronous copies of its amplitudes (unless the pass
 // starts from |+>), slot s = tid, tid + nthr, ... in order, so consecutive threads copy
-// consecutive amplitudes, and of its costs: FP64 costs per slot, byte costs in runs of
-// 4-16 bytes (a 16-byte copy holds 16 costs; a high chunk's row holds W costs).
+// consecutive amplitudes, and of its costs: FP64 costs per slot, byte costs as one
+// contiguous run in 16-byte copies (I.cost is the transposed array in high passes).
 // Mem::cp16(dst, x) copies amplitude x; CostMem::cpw(dst, x) the FP64 cost of amplitude
 // x; CostMem::cpb(dst, x, bytes) bytes byte costs from amplitude x (x a multiple of bytes).
 template <class CostT, class Mem, class CostMem>
@@ -381,34 +386,23 @@ ORKAN_HD void qaoa_fill(const QaoaPass& P, const QaoaTables& T, const QaoaInst& 
             if (!pl.init) psi.cp16(S.vb + qaoa_pad(e), x0 + e);
             if constexpr (!kBytes) cost.cpw(S.cw + qaoa_pad(e), x0 + e);
         }
-        if constexpr (kBytes) {
-            if (cnt >= 16 || P.kind == kQaoaFull) {   // 16 costs per copy (whole 16-byte units)
-                for (unsigned e = 16 * tid; e < cnt || (e == 0 && cnt < 16); e += 16 * nthr)
-                    cost.cpb(S.cb + e, x0 + e, 16);
-            } else if (tid == 0) {                    // a chunk of 1-8 costs: one copy
-                if (cnt >= 4) cost.cpb(S.cb, x0, cnt);
-                else cost.cpb(S.cb, x0 & ~idx_t(3), 4);
-            }
+    } else {
+        const unsigned R = I.n - P.C, lw = qaoa_logw(I.n, P.C);
+        for (unsigned e = tid; e < cnt; e += nthr) {
+            const unsigned s = qaoa_high_slot(e, R, lw, 0, 0);
+            const idx_t x = qaoa_index(I.n, P.C, P.kind, chunk, s);
+            if (!pl.init) psi.cp16(S.vb + qaoa_pad(s), x);
+            if constexpr (!kBytes) cost.cpw(S.cw + qaoa_pad(s), x);
         }
-        return;
     }
-    const unsigned R = I.n - P.C, lw = qaoa_logw(I.n, P.C);
-    for (unsigned e = tid; e < cnt; e += nthr) {
-        const unsigned s = qaoa_high_slot(e, R, lw, 0, 0);
-        const idx_t x = qaoa_index(I.n, P.C, P.kind, chunk, s);
-        if (!pl.init) psi.cp16(S.vb + qaoa_pad(s), x);
-        if constexpr (!kBytes) cost.cpw(S.cw + qaoa_pad(s), x);
-    }
-    if constexpr (kBytes) {
-        // row r's W costs start at amplitude r 2^C + chunk W: runs of min(W, 16) bytes, or the
-        // row's aligned 4-byte word when W < 4
-        const unsigned W = 1u << lw, run = W >= 16 ? 16u : (W >= 4 ? W : 4u);
-        const unsigned per_row = W >= 16 ? W / 16 : 1u;
-        for (unsigned e = tid; e < (per_row << R); e += nthr) {
-            const unsigned row = e / per_row, k = e % per_row;
-            const idx_t x = ((idx_t)row << P.C) + (chunk << lw) + (idx_t)k * run;
-            if (W >= 4) cost.cpb(S.cb + row * W + k * run, x, run);
-            else cost.cpb(S.cb + 4 * row, x & ~idx_t(3), 4);
+    if constexpr (kBytes) {                        // one contiguous run (transposed in high passes)
+        const idx_t x0 = P.kind == kQaoaFull ? 0 : chunk << P.C;
+        if (cnt >= 16 || P.kind == kQaoaFull) {   // 16 costs per copy (whole 16-byte units)
+            for (unsigned e = 16 * tid; e < cnt || (e == 0 && cnt < 16); e += 16 * nthr)
+                cost.cpb(S.cb + e, x0 + e, 16);
+        } else if (tid == 0) {                    // a chunk of 1-8 costs: one copy
+            if (cnt >= 4) cost.cpb(S.cb, x0, cnt);
+            else cost.cpb(S.cb, x0 & ~idx_t(3), 4);
         }
     }
 }
@@ -438,7 +432,7 @@ ORKAN_HD void qaoa_group(const QaoaPass& P, const QaoaTables& T, const QaoaInst&
             if constexpr (std::is_same<CostT, double>::value) {
                 return S.cw[p0 + j * D];
             } else {
-                return S.cb[qaoa_cost_index(P.kind, P.C, R, lw, chunk, base | (j << B0))];
+                return S.cb[qaoa_cost_index(P.kind, P.C, chunk, base | (j << B0))];
             }
         };
         double2 v[NV];

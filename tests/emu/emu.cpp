@@ -204,6 +204,14 @@ int run_qaoa(unsigned n, const CostT* cost, unsigned p, const double* gamma, con
     const EmuMem mem{reinterpret_cast<double2*>(psi), dim, reads, writes, oob};
     const idx_t clen = sizeof(CostT) == 1 ? ((dim + 15) / 16) * 16 : dim;
     const EmuCost<CostT> cmem{cost, clen, oob};
+    // byte costs of the high passes: the transposed array (qaoa_cost_t_index), as the batch
+    // context builds it for the chunk size
+    std::vector<CostT> cost_t;
+    if (sizeof(CostT) == 1 && !full) {
+        cost_t.assign((size_t)clen, CostT(0));
+        for (idx_t x = 0; x < dim; ++x) cost_t[(size_t)qaoa_cost_t_index(n, C, x)] = cost[x];
+    }
+    const EmuCost<CostT> cmem_t{cost_t.empty() ? cost : cost_t.data(), clen, oob};
     const unsigned npass = full ? 1 : p + 1;
     for (unsigned j = 0; j < npass && j <= upto; ++j) {
         QaoaPass P;
@@ -222,8 +230,11 @@ int run_qaoa(unsigned n, const CostT* cost, unsigned p, const double* gamma, con
         const QaoaPlan& pl = P.plan;
         std::vector<unsigned char> smem(qaoa_smem_bytes<CostT>(P.C, nthr, 1));
         const QaoaSmem<CostT> S = qaoa_smem_at<CostT>(smem.data(), P.C, nthr, 1, 0);
+        const bool transposed = P.kind == kQaoaHigh && !cost_t.empty();
+        I.cost = transposed ? static_cast<const void*>(cost_t.data()) : static_cast<const void*>(cost);
+        const EmuCost<CostT>& cm = transposed ? cmem_t : cmem;
         for (idx_t w = 0; w < P.items; ++w) {
-            for (unsigned t = 0; t < nthr; ++t) qaoa_fill<CostT>(P, T, I, pl, mem, cmem, w, S, t, nthr);
+            for (unsigned t = 0; t < nthr; ++t) qaoa_fill<CostT>(P, T, I, pl, mem, cm, w, S, t, nthr);
             for (unsigned st = 0; st < qaoa_stages(pl); ++st)
                 for (unsigned t = 0; t < nthr; ++t) qaoa_stage<CostT>(P, T, I, pl, mem, w, st, S, t, nthr);
         }
