@@ -37,8 +37,9 @@ typedef struct orkan_qaoa orkan_qaoa_t;
  *   mem_budget         device bytes the batch may use for state vectors (0: 60 % of the free
  *                      memory after the cost vectors); instances are evaluated in waves that fit
  *   flags              ORKAN_QAOA_* flags
- * Instances with the same qubit count, edge list and weights share one resident cost vector.
- * All arrays are host arrays, copied. */
+ * Instances with the same qubit count, edge list and weights share one resident cost vector
+ * (2^n bytes for byte costs, plus a transposed copy of the same size that the high passes
+ * read; 2^n doubles for FP64 costs).  All arrays are host arrays, copied. */
 int orkan_qaoa_create(orkan_qaoa_t **out, unsigned count, const unsigned *n_qubits, const unsigned *edge_offsets,
                       const unsigned *edges, const double *weights, unsigned p, unsigned long long mem_budget,
                       unsigned flags);
